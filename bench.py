@@ -1,0 +1,398 @@
+#!/usr/bin/env python3
+"""Benchmark: hash-join probe throughput on one B200 (and N replicas).
+
+Workload (the join configuration): build side 2^22 unique int32 keys (a
+seeded permutation of 0..2^22-1) with int32 payload uniform [0, 2^20);
+probe side 2^26 int32 keys, 90% drawn uniformly from the build keys and 10%
+uniform in [2^22, 2^31), with int32 payload uniform [0, 2^20).  One step is
+one probe pass: open -> consume(2^26 rows) -> close through the operator API,
+producing COUNT(matches) and int64 SUM(build payload + probe payload).  The
+hash table is built once, outside the timed steps.
+
+  value : probe tuples/s with the probe columns resident in HBM
+  e2e   : the same through the C ABI from pinned HOST memory: per step the
+          probe columns are written into pool buffers (H2D) and consumed
+          buffer by buffer, the result read back by close()
+
+Multi-GPU: one process per GPU, each an independent replica of the
+workload (the probe shards with no exchange); value = all ranks' tuples /
+the slowest rank's time.  `--impl reference` times the CPU restatement of
+the reference's chained-table join (src/main8.cu:84-103) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "multigpu-vector_b200"))
+
+BUILD_ROWS = 1 << 22
+PROBE_ROWS = 1 << 26
+HIT = 3865470566  # 0.9 * 2^32
+SEED_B, SEED_P = 0x5EED0002, 0x5EED0003
+METRIC = "join-probe tuples/s, % of HBM peak; batched queries/s & p99 vs plain"
+BYTES_PER_TUPLE = 8  # probe key + probe payload, read once
+WORKLOAD = ("hash join probe: build 2^22 unique int32 keys (seeded permutation) + int32 payload "
+            "U[0,2^20); probe 2^26 int32 keys (90% build keys, 10% U[2^22,2^31)) + int32 payload "
+            "U[0,2^20); COUNT + int64 SUM(build_payload + probe_payload)")
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def probe_traffic_per_launch():
+    """DRAM bytes per probe launch from the committed ncu summary, if any."""
+    p = os.path.join(HERE, "profiles", "join_probe_traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0, t1):
+        """Host-clock window of the timed region."""
+        self.window = (t0, t1)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        w = getattr(self, "window", None)
+        inside = [ln for t, ln in self.lines if w and w[0] <= t <= w[1]]
+        scope = "timed region"
+        if not inside:  # region shorter than the sampling period: use the whole run
+            inside = [ln for _, ln in self.lines]
+            scope = "warm-up + timed region"
+        for ln in inside:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm), "scope": scope}
+
+
+def cpu_probe_baseline(bk, bp, pk, pp, threads):
+    """Oracle chained-table probe (src/main8.cu:84-103 restated) on host cores."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import pyoracle as po
+
+    chain = po.Chain(bk, bp)  # build once, not timed (the GPU table is built untimed too)
+    t0 = time.perf_counter()
+    res = chain.probe_agg_mt(pk, pp, threads)
+    dt = time.perf_counter() - t0
+    return pk.size / dt, dt, res
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import numpy as np
+    import pyoracle as po
+
+    nb, npb = BUILD_ROWS, PROBE_ROWS
+    bk = po.gen_perm(nb, SEED_B)
+    bp = po.gen_uniform(nb, SEED_B, 1, 0, 1 << 20)
+    sample = min(npb, args.cpu_sample)
+    pk, _ = po.gen_probe_keys(sample, SEED_P, SEED_B, nb, HIT, nb, (1 << 31) - nb)
+    pp = po.gen_uniform(sample, SEED_P, 2, 0, 1 << 20)
+    threads = os.cpu_count() or 1
+    chain = po.Chain(bk, bp)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        chain.probe_agg_mt(pk, pp, threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    ms = 1000.0 * statistics.median(times)
+    v = sample / (ms / 1000.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "build_rows": nb, "probe_rows": npb, "probe_rows_per_step_sample": sample},
+        "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
+                         "sample": f"probe of {sample} rows per step against the full 2^22-key chained table "
+                                   f"(built once, untimed), {threads} threads"},
+        "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mgv", choices=["mgv", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=1 << 24)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--load-factor", type=float, default=0.5)
+    ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
+    ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--probe-kernel", type=int, default=None, help="0 auto, 1 register prefetch, 2 staged")
+    ap.add_argument("--rows-per-thread", type=int, default=None)
+    ap.add_argument("--stages", type=int, default=None)
+    ap.add_argument("--ctas-per-sm", type=int, default=None)
+    ap.add_argument("--settle-s", type=float, default=1.0, help="untimed steps before timing, in seconds")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import mgv
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    ctx = mgv.Context(local)
+    tune = {k: v for k, v in (("probe_kernel", args.probe_kernel), ("probe_rows_per_thread", args.rows_per_thread),
+                              ("probe_stages", args.stages), ("probe_ctas_per_sm", args.ctas_per_sm)) if v is not None}
+    if tune:
+        ctx.set_tuning(**tune)
+    tuning = ctx.tuning()
+    stream = torch.cuda.Stream()
+    nb, npb = args.build_rows, args.probe_rows
+
+    with torch.cuda.stream(stream):
+        bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+        bp = torch.empty(nb, dtype=torch.int32, device="cuda")
+        pk = torch.empty(npb, dtype=torch.int32, device="cuda")
+        pp = torch.empty(npb, dtype=torch.int32, device="cuda")
+    ctx.gen_perm(bk, nb, SEED_B, stream=stream)
+    ctx.gen_uniform(bp, nb, SEED_B, 1, 0, 1 << 20, stream=stream)
+    hits = ctx.gen_probe_keys(pk, npb, SEED_P, SEED_B, nb, HIT, nb, (1 << 31) - nb, stream=stream)
+    ctx.gen_uniform(pp, npb, SEED_P, 2, 0, 1 << 20, stream=stream)
+
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb, args.load_factor)
+    tb0 = torch.cuda.Event(enable_timing=True)
+    tb1 = torch.cuda.Event(enable_timing=True)
+    tb0.record(stream)
+    bhead.open(stream)
+    bhead.consume_columns([bk, bp], nb, stream)
+    bhead.close(stream)
+    tb1.record(stream)
+    stream.synchronize()
+    build_ms = tb0.elapsed_time(tb1)
+    info = hb.result()
+
+    def step():
+        probe.open(stream)
+        probe.consume_columns([pk, pp], npb, stream)
+        probe.close(stream)
+
+    for _ in range(args.warmup):
+        step()
+    cnt, s = agg.result()
+    assert cnt == hits, f"match count {cnt} != generated hits {hits}"
+
+    # per-launch probe kernel time (events bracket the single probe launch)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        # settle clocks (and let the sampler start) before the timed region
+        t_settle = time.time()
+        while time.time() - t_settle < args.settle_s:
+            step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = ctx.launches
+        h0 = time.time()
+        start.record(stream)
+        for i in range(args.steps):
+            probe.open(stream)
+            kev[i][0].record(stream)
+            probe.consume_columns([pk, pp], npb, stream)
+            kev[i][1].record(stream)
+            probe.close(stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+        clk.mark(h0, time.time())
+    launches = ctx.launches - launches0
+    if dist:
+        dist.barrier()
+    elapsed = start.elapsed_time(end) / 1000.0
+    kernel_s = statistics.mean(a.elapsed_time(b) for a, b in kev) / 1000.0
+    if dist:
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    # ---- end to end through the C ABI from pinned host memory -------------
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, (cnt, s))
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = min(npb, args.cpu_sample)
+        threads = os.cpu_count() or 1
+        v, dt, res = cpu_probe_baseline(bk.cpu().numpy(), bp.cpu().numpy(), pk[:sample].cpu().numpy(),
+                                        pp[:sample].cpu().numpy(), threads)
+        cpu = {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
+               "sample": f"first {sample} probe rows against the full 2^22-key chained table "
+                         f"(built once, untimed); {dt:.2f} s on {threads} threads"}
+    return finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank,
+                  dist, (probe, agg, bhead, hb), nb, npb, tuning)
+
+
+def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, want):
+    cap = mgv.DEFAULT_BUFFER_ROWS
+    nbuf = (npb + cap - 1) // cap
+    pool = mgv.Pool(ctx, nbuf, cap, 2)
+    bufs = [pool.acquire() for _ in range(nbuf)]
+    hpk = pk.cpu().pin_memory()
+    hpp = pp.cpu().pin_memory()
+    e2e_steps = max(1, args.e2e_steps)
+
+    def e2e_step():
+        probe.open(stream)
+        for j, b in enumerate(bufs):
+            lo = j * cap
+            m = min(cap, npb - lo)
+            mgv.buffer_write(b, 0, hpk.data_ptr() + 4 * lo, m, stream)
+            mgv.buffer_write(b, 1, hpp.data_ptr() + 4 * lo, m, stream)
+            probe.consume(b, stream)
+        probe.close(stream)
+
+    e2e_step()
+    assert agg.result() == want
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1000.0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * npb * e2e_steps / e2e_s
+    for b in bufs:
+        pool.release(b)
+    pool.destroy()
+    return {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": 8 * npb, "d2h_bytes_per_step": 16,
+            "path": "mgv_buffer_write (pinned host -> pool buffer) + mgv_op_consume per 4Mi-row buffer"}
+
+
+def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank, dist,
+           ops, nb, npb, tuning):
+    value = world * npb * args.steps / elapsed
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_TUPLE * npb / kernel_s / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD, "build_rows": nb, "probe_rows": npb, "load_factor": args.load_factor,
+            "table_bytes": int(info.table_bytes), "build_ms": build_ms, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2: 512 MiB of probe columns streamed per step; the hash table "
+                  "stays L2-resident by design",
+            "step": "open -> consume(2^26 rows) -> close (COUNT + SUM read back)",
+            "tuning": {"probe_kernel": tuning.probe_kernel, "rows_per_thread": tuning.probe_rows_per_thread,
+                       "stages": tuning.probe_stages, "ctas_per_sm": tuning.probe_ctas_per_sm},
+        },
+        "hbm_peak_frac": achieved / peak,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "kernel_ms": kernel_s * 1000.0,
+                     "algorithmic_bytes_per_launch": BYTES_PER_TUPLE * npb,
+                     "traffic": probe_traffic_per_launch()},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "result": {"count": cnt, "sum": s},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for o in ops:
+        o.destroy()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,279 @@
+/*
+ * mgv.h -- C ABI of the B200 vector-at-a-time operator pipeline.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, no C++ or torch types.
+ * Every call returns an mgv_status; nothing here calls exit() or aborts
+ * (the reference's gpu() macro exits on any CUDA error, src/common.cuh:12-23).
+ * Device pointers are CUDA device addresses on the context's device;
+ * `stream` arguments are cudaStream_t values (NULL = the context's stream).
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the reference project).
+ */
+#ifndef MGV_H_
+#define MGV_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGV_MAX_COLS 8
+/* Rows per pool buffer by default: DEFAULT_BUFF_CAP, src/common.cuh:8-10. */
+#define MGV_DEFAULT_BUFFER_ROWS (4u * 1024u * 1024u)
+
+typedef enum mgv_status {
+    MGV_OK = 0,
+    MGV_EINVAL = 1,      /* bad argument                                  */
+    MGV_ENOMEM = 2,      /* allocation failed / pool, table or output full */
+    MGV_ETIMEDOUT = 3,   /* a bounded wait ran out                         */
+    MGV_ECUDA = 4,       /* CUDA runtime error (see mgv_last_error_string) */
+    MGV_EDEVICE = 5,     /* a kernel reported an error word                */
+    MGV_ESTATE = 6,      /* call not valid in the object's current state   */
+    MGV_EDRAINED = 7,    /* pool empty and no producer registered          */
+    MGV_EUNSUPPORTED = 8 /* operator chain has no kernel                   */
+} mgv_status;
+
+typedef struct mgv_ctx mgv_ctx;
+typedef struct mgv_pool mgv_pool;
+typedef struct mgv_op mgv_op;
+
+/* A vector buffer: up to MGV_MAX_COLS int32 columns of `capacity` rows in
+ * device memory, `rows` of them valid.  Replaces buffer<int32_t, 4Mi>
+ * (src/buffer.cuh:15-31: cnt, data, device), extended to several columns. */
+typedef struct mgv_buffer {
+    int32_t *cols[MGV_MAX_COLS];
+    uint32_t ncols;
+    uint32_t rows;
+    uint32_t capacity;
+    uint32_t id;
+    int32_t device;
+    uint32_t reserved;
+} mgv_buffer;
+
+/* ---- errors ----------------------------------------------------------- */
+
+const char *mgv_status_string(mgv_status s);
+/* Detail of the last failing call on this thread. */
+const char *mgv_last_error_string(void);
+
+/* ---- context ---------------------------------------------------------- */
+
+typedef struct mgv_ctx_info {
+    int32_t device;
+    int32_t sm_count;
+    uint64_t l2_bytes;
+    uint64_t hbm_bytes;
+    int32_t cc_major, cc_minor;
+    char name[64];
+} mgv_ctx_info;
+
+/* Replaces the per-device set-up of buffer_manager::init
+ * (src/buffer_manager.cu:38-61): device selection and a context stream. */
+mgv_status mgv_ctx_create(int device, mgv_ctx **out);
+mgv_status mgv_ctx_destroy(mgv_ctx *ctx);
+mgv_status mgv_ctx_info_get(mgv_ctx *ctx, mgv_ctx_info *out);
+/* Waits for `stream`, then reports and clears the device error word. */
+mgv_status mgv_ctx_sync(mgv_ctx *ctx, void *stream);
+/* Number of mgv kernel launches issued by this context so far. */
+uint64_t mgv_ctx_launches(mgv_ctx *ctx);
+
+/* Kernel tuning of a context (the reference fixes its launch shapes per
+ * driver, e.g. <<<128, 1024>>> in src/main9.cu:593-594; here they are
+ * runtime parameters, set by the caller or by the autotuner). */
+typedef struct mgv_tuning {
+    uint32_t probe_kernel;          /* 0 auto, 1 register prefetch, 2 bulk-copy staged */
+    uint32_t probe_rows_per_thread; /* staged probe: 4 or 8 rows per thread per tile   */
+    uint32_t probe_stages;          /* staged probe: 2, 4 or 6 tiles in flight         */
+    uint32_t probe_ctas_per_sm;     /* 0 = as many as fit; 3 with 4 rows per thread
+                                       selects the 3-CTA register budget               */
+    float default_load_factor;      /* hash_build tables whose desc gives 0            */
+    uint32_t reserved[3];
+} mgv_tuning;
+
+mgv_status mgv_ctx_set_tuning(mgv_ctx *ctx, const mgv_tuning *t);
+mgv_status mgv_ctx_get_tuning(mgv_ctx *ctx, mgv_tuning *t);
+
+/* ---- buffer pool (buffer_pool / buffer_manager) ------------------------ */
+
+typedef struct mgv_pool_stats {
+    uint32_t nbuffers;
+    uint32_t capacity;
+    uint32_t ncols;
+    uint32_t available;     /* buffers on the device free stack           */
+    uint32_t host_cached;   /* buffers held in the host-side cache        */
+    uint32_t producers;
+    uint64_t bytes;
+} mgv_pool_stats;
+
+/* One device slab carved into `nbuffers` buffers of `ncols` x `capacity`
+ * int32 (buffer_manager::init's cudaMallocPitch slab,
+ * src/buffer_manager.cu:98-134), with a device free stack
+ * (src/threadsafe_device_stack.cuh:19-87, src/lockfree_stack.cuh:19-208). */
+mgv_status mgv_pool_create(mgv_ctx *ctx, uint32_t nbuffers, uint32_t capacity,
+                           uint32_t ncols, mgv_pool **out);
+mgv_status mgv_pool_destroy(mgv_pool *pool);
+/* Host acquire: buffer_manager::h_get_buffer (src/buffer_manager.cuh:78-94),
+ * batching device pops through a host cache, with the bounded wait of
+ * buffer_pool::acquire_buffer_blocked_unsafe (src/buffer_pool.cuh:83-96):
+ * MGV_EDRAINED when the pool is empty and no producer is registered,
+ * MGV_ETIMEDOUT when a producer is registered but nothing came back within
+ * timeout_us. */
+mgv_status mgv_buffer_acquire(mgv_pool *pool, uint32_t timeout_us, mgv_buffer **out);
+/* Host release: buffer_manager::release_buffer (src/buffer_manager.cuh:96-118). */
+mgv_status mgv_buffer_release(mgv_pool *pool, mgv_buffer *buf);
+/* Copy `rows` int32 from host or device memory into column `col` and set
+ * the buffer's row count: buffer_manager::overwrite
+ * (src/buffer_manager.cu:214-218) / buffer_inspector::overwrite
+ * (src/buffer.cuh:190-196).  Asynchronous on `stream`; with stream NULL
+ * the copy has completed when the call returns (blocking = true). */
+mgv_status mgv_buffer_write(mgv_buffer *buf, uint32_t col, const void *src, uint32_t rows,
+                            void *stream);
+/* Copy `rows` of column `col` to host or device memory and wait for it:
+ * buffer_inspector::read (src/buffer.cuh:198-202). */
+mgv_status mgv_buffer_read(const mgv_buffer *buf, uint32_t col, void *dst, uint32_t rows,
+                           void *stream);
+/* buffer_pool::register_producer / unregister_producer
+ * (src/buffer_pool.cuh:136-165). */
+mgv_status mgv_pool_register_producer(mgv_pool *pool);
+mgv_status mgv_pool_unregister_producer(mgv_pool *pool);
+mgv_status mgv_pool_stats_get(mgv_pool *pool, mgv_pool_stats *out);
+
+/* ---- operators -------------------------------------------------------- */
+/*
+ * Operators form push chains as in the reference (d_operator_t with a
+ * parent pointer, src/operators/operator.cuh:42-86): rows pushed into an
+ * operator flow to its parent.  A chain from the operator that receives
+ * data up to its terminal (aggregate, groupby, hash_build, sink, partition)
+ * runs as ONE fused kernel per consume call; there is no per-row dispatch.
+ *
+ * Column numbering: the rows entering a chain carry the consumed buffer's
+ * columns 0..ncols-1; select keeps them all; hash_probe appends the
+ * matching build row's payload as column `ncols` (one output row per
+ * match).
+ */
+
+/* unstable_select with less_eq_than (src/operators/select3.cuh:10-48):
+ * keeps rows with cols[col] <= bound (signed compare). */
+typedef struct mgv_select_desc {
+    uint32_t col;
+    int32_t bound;
+} mgv_select_desc;
+
+/* aggregation (src/operators/aggregation.cu:5-66), widened: COUNT(*) and
+ * int64 SUM(cols[sum_col_a] + cols[sum_col_b]); -1 leaves a term out. */
+typedef struct mgv_aggregate_desc {
+    int32_t sum_col_a;
+    int32_t sum_col_b;
+} mgv_aggregate_desc;
+
+typedef struct mgv_agg_result {
+    int64_t count;
+    int64_t sum;
+} mgv_agg_result;
+
+/* hashjoin_builder (src/operators/hashjoin.cu:40-60), as an open-addressing
+ * table of 32-byte buckets (4 {key, payload} slots, one L2 sector).
+ * expected_rows sizes the table; load_factor in (0, 0.95] (0 = default
+ * 0.5); payload_col -1 stores payload 0. */
+typedef struct mgv_hash_build_desc {
+    uint32_t key_col;
+    int32_t payload_col;
+    uint64_t expected_rows;
+    float load_factor;
+    uint32_t reserved;
+} mgv_hash_build_desc;
+
+typedef struct mgv_hash_build_info {
+    uint64_t rows;            /* rows inserted                               */
+    uint64_t nbuckets;
+    uint64_t table_bytes;
+    uint64_t reserved_key_rows; /* build rows whose key is INT32_MIN         */
+    uint32_t has_duplicates;  /* 1 if some key was inserted more than once   */
+    uint32_t reserved;
+} mgv_hash_build_info;
+
+/* hashjoin probe (src/operators/hashjoin.cu:134-182): each row is matched
+ * against every build row with an equal key (duplicates all match). */
+typedef struct mgv_hash_probe_desc {
+    uint32_t key_col;
+    uint32_t reserved;
+    mgv_op *build;            /* a closed hash_build operator              */
+} mgv_hash_probe_desc;
+
+/* Materialises rows into buffers of `pool` (the pool's ncols columns are
+ * filled from the incoming columns 0..ncols-1): the reference's
+ * gpu_to_cpu output buffers with swap-on-full
+ * (src/operators/gpu_to_cpu.cu:41-105, src/buffer_manager.cuh:147-176). */
+typedef struct mgv_sink_desc {
+    mgv_pool *pool;
+    uint32_t max_buffers;     /* 0 = as many as the pool has               */
+    uint32_t reserved;
+} mgv_sink_desc;
+
+mgv_status mgv_op_create_select(mgv_ctx *ctx, const mgv_select_desc *desc, mgv_op *parent,
+                                mgv_op **out);
+mgv_status mgv_op_create_aggregate(mgv_ctx *ctx, const mgv_aggregate_desc *desc, mgv_op **out);
+mgv_status mgv_op_create_hash_build(mgv_ctx *ctx, const mgv_hash_build_desc *desc, mgv_op **out);
+mgv_status mgv_op_create_hash_probe(mgv_ctx *ctx, const mgv_hash_probe_desc *desc,
+                                    mgv_op *parent, mgv_op **out);
+mgv_status mgv_op_create_sink(mgv_ctx *ctx, const mgv_sink_desc *desc, mgv_op **out);
+/* Operators are destroyed explicitly (the reference never frees them,
+ * src/operators/operator.cu:161-163); parents are not destroyed. */
+mgv_status mgv_op_destroy(mgv_op *op);
+
+/* d_operator_t::open (src/operators/operator.cu:126-135): opens the
+ * parents first, then resets this operator's device state. */
+mgv_status mgv_op_open(mgv_op *op, void *stream);
+/* launch_consume_pipeline over one buffer (src/operators/exchange.cu:160-194):
+ * every valid row of `buf` is pushed through the chain in one launch. */
+mgv_status mgv_op_consume(mgv_op *op, const mgv_buffer *buf, void *stream);
+/* The same over device-resident columns of any length (the reference's
+ * generator aliasing a user array into buffers, src/operators/generators.cu:55-90). */
+mgv_status mgv_op_consume_columns(mgv_op *op, const int32_t *const *cols, uint32_t ncols,
+                                  uint64_t rows, void *stream);
+/* d_operator_t::close (src/operators/operator.cu:150-159): flushes, closes
+ * the parents, waits for the stream and reports device errors. */
+mgv_status mgv_op_close(mgv_op *op, void *stream);
+/* Result of a closed terminal operator, copied to host memory:
+ *   aggregate  -> mgv_agg_result
+ *   hash_build -> mgv_hash_build_info
+ *   sink       -> uint64_t row count
+ * `needed` (may be NULL) receives the size in bytes. */
+mgv_status mgv_op_result(mgv_op *op, void *out, size_t bytes, size_t *needed);
+
+/* Rows of a closed sink: copies up to `max_rows` rows of column `col`
+ * (in buffer order) into dst (host or device memory). */
+mgv_status mgv_sink_read(mgv_op *sink, uint32_t col, int32_t *dst, uint64_t max_rows,
+                         uint64_t *rows);
+
+/* ---- seeded synthetic columns ------------------------------------------ */
+/*
+ * Fill device memory with seeded columns; value i is a pure function of
+ * (seed, stream_id, i), identical to the CPU oracle's generator.  No
+ * reference counterpart: the reference fills host arrays with unseeded
+ * rand() / mt19937 (src/main8.cu:169, src/main9.cu:556-566).
+ */
+/* Uniform int32 in [lo, lo + range), range in [1, 2^32]. */
+mgv_status mgv_gen_uniform(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint32_t stream_id,
+                           int64_t lo, uint64_t range, void *stream);
+/* A seeded permutation of 0..n-1. */
+mgv_status mgv_gen_perm(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, void *stream);
+/* Join probe keys: with probability hit_num/2^32 a uniformly chosen key of
+ * the permutation mgv_gen_perm(build_seed, nbuild), else uniform in
+ * [miss_lo, miss_lo + miss_range).  *hits (may be NULL) receives how many
+ * rows took the first branch. */
+mgv_status mgv_gen_probe_keys(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint64_t build_seed,
+                              uint64_t nbuild, uint32_t hit_num, int64_t miss_lo, uint64_t miss_range,
+                              uint64_t *hits, void *stream);
+/* Zipf(s) group ids in [0, groups), 0 the most frequent. */
+mgv_status mgv_gen_zipf(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint32_t stream_id,
+                        uint32_t groups, double s, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGV_H_ */

@@ -1,0 +1,703 @@
+// capi.cu -- the extern "C" boundary (include/mgv.h): contexts, pools,
+// buffers and the operator graph with open / consume / close.
+//
+// The operator graph mirrors d_operator_t (src/operators/operator.cuh:42-86,
+// src/operators/operator.cu:114-159): operators hold a parent pointer, open()
+// opens parents first, close() closes them after the operator's own flush.
+// Unlike the reference, a consume() call does not dispatch per 128-row
+// vector through a variant: the chain below the consuming operator is
+// matched to one fused kernel (kernels.cu) and launched once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "device_common.cuh"
+#include "mgv_internal.h"
+
+using namespace mgv;
+
+namespace mgv {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+mgv_status fail(mgv_status s, const std::string& msg) {
+    set_last_error(msg);
+    return s;
+}
+
+mgv_status cuda_fail(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    set_last_error(m);
+    if (e == cudaErrorMemoryAllocation) return MGV_ENOMEM;
+    return MGV_ECUDA;
+}
+
+}  // namespace mgv
+
+static cudaStream_t pick_stream(Context* ctx, void* stream) {
+    return stream ? (cudaStream_t)stream : ctx->stream;
+}
+
+// Reads and clears the context's device error word after `s` completes.
+static mgv_status check_device(Context* ctx, cudaStream_t s) {
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+    uint32_t h[2] = {0, 0};
+    MGV_CUDA_TRY(cudaMemcpy(h, ctx->d_err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h[0] == 0) return MGV_OK;
+    MGV_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(h)));
+    char msg[128];
+    std::snprintf(msg, sizeof(msg), "device error word %u (site %u)", h[0], h[1]);
+    if (h[0] == MGV_ENOMEM) return fail(MGV_ENOMEM, std::string(msg) + ": table, pool or output full");
+    if (h[0] == MGV_ETIMEDOUT) return fail(MGV_ETIMEDOUT, std::string(msg) + ": bounded wait ran out");
+    return fail(MGV_EDEVICE, msg);
+}
+
+extern "C" {
+
+const char* mgv_status_string(mgv_status s) {
+    switch (s) {
+        case MGV_OK: return "ok";
+        case MGV_EINVAL: return "invalid argument";
+        case MGV_ENOMEM: return "out of memory / capacity";
+        case MGV_ETIMEDOUT: return "timed out";
+        case MGV_ECUDA: return "CUDA error";
+        case MGV_EDEVICE: return "device error";
+        case MGV_ESTATE: return "invalid state";
+        case MGV_EDRAINED: return "pool drained";
+        case MGV_EUNSUPPORTED: return "unsupported operator chain";
+    }
+    return "unknown status";
+}
+
+const char* mgv_last_error_string(void) { return g_last_error.c_str(); }
+
+// ---- context ---------------------------------------------------------------
+
+mgv_status mgv_ctx_create(int device, mgv_ctx** out) {
+    if (!out) return fail(MGV_EINVAL, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    MGV_CUDA_TRY(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(MGV_EINVAL, "no such device");
+    MGV_CUDA_TRY(cudaSetDevice(device));
+    mgv_ctx* c = new (std::nothrow) mgv_ctx();
+    if (!c) return fail(MGV_ENOMEM, "host allocation");
+    c->device = device;
+    cudaError_t e = cudaGetDeviceProperties(&c->prop, device);
+    // A blocking stream: work on it is ordered with the legacy default
+    // stream, so callers that use the default stream need no extra sync.
+    if (e == cudaSuccess) e = cudaStreamCreate(&c->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 2 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        if (c->d_err) cudaFree(c->d_err);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return cuda_fail(e, "mgv_ctx_create");
+    }
+    *out = c;
+    return MGV_OK;
+}
+
+mgv_status mgv_ctx_destroy(mgv_ctx* ctx) {
+    if (!ctx) return MGV_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->d_err);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return MGV_OK;
+}
+
+mgv_status mgv_ctx_info_get(mgv_ctx* ctx, mgv_ctx_info* out) {
+    if (!ctx || !out) return fail(MGV_EINVAL, "NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    out->device = ctx->device;
+    out->sm_count = ctx->prop.multiProcessorCount;
+    out->l2_bytes = (uint64_t)ctx->prop.l2CacheSize;
+    out->hbm_bytes = (uint64_t)ctx->prop.totalGlobalMem;
+    out->cc_major = ctx->prop.major;
+    out->cc_minor = ctx->prop.minor;
+    std::snprintf(out->name, sizeof(out->name), "%s", ctx->prop.name);
+    return MGV_OK;
+}
+
+mgv_status mgv_ctx_sync(mgv_ctx* ctx, void* stream) {
+    if (!ctx) return fail(MGV_EINVAL, "ctx is NULL");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    return check_device(ctx, pick_stream(ctx, stream));
+}
+
+uint64_t mgv_ctx_launches(mgv_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+mgv_status mgv_ctx_set_tuning(mgv_ctx* ctx, const mgv_tuning* t) {
+    if (!ctx || !t) return fail(MGV_EINVAL, "NULL argument");
+    if (t->probe_kernel > 2) return fail(MGV_EINVAL, "probe_kernel must be 0, 1 or 2");
+    if (t->probe_rows_per_thread != 4 && t->probe_rows_per_thread != 8)
+        return fail(MGV_EINVAL, "probe_rows_per_thread must be 4 or 8");
+    if (t->probe_stages != 2 && t->probe_stages != 4 && t->probe_stages != 6)
+        return fail(MGV_EINVAL, "probe_stages must be 2, 4 or 6");
+    if (t->probe_ctas_per_sm > 32) return fail(MGV_EINVAL, "probe_ctas_per_sm out of range");
+    if (!(t->default_load_factor > 0.0f && t->default_load_factor <= 0.95f))
+        return fail(MGV_EINVAL, "default_load_factor must be in (0, 0.95]");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tuning = *t;
+    return MGV_OK;
+}
+
+mgv_status mgv_ctx_get_tuning(mgv_ctx* ctx, mgv_tuning* t) {
+    if (!ctx || !t) return fail(MGV_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *t = ctx->tuning;
+    return MGV_OK;
+}
+
+// ---- pool ------------------------------------------------------------------
+
+mgv_status mgv_pool_create(mgv_ctx* ctx, uint32_t nbuffers, uint32_t capacity, uint32_t ncols,
+                           mgv_pool** out) {
+    if (!ctx || !out) return fail(MGV_EINVAL, "NULL argument");
+    *out = nullptr;
+    if (nbuffers == 0 || nbuffers >= kNil - 1) return fail(MGV_EINVAL, "nbuffers out of range");
+    if (capacity == 0 || capacity % 128 != 0)
+        return fail(MGV_EINVAL, "capacity must be a positive multiple of 128 rows");
+    if (ncols == 0 || ncols > MGV_MAX_COLS) return fail(MGV_EINVAL, "ncols out of range");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_pool* p = new (std::nothrow) mgv_pool();
+    if (!p) return fail(MGV_ENOMEM, "host allocation");
+    p->ctx = ctx;
+    p->nbuffers = nbuffers;
+    p->capacity = capacity;
+    p->ncols = ncols;
+    const size_t slab_bytes = (size_t)nbuffers * ncols * capacity * sizeof(int32_t);
+    cudaError_t e = cudaMalloc(&p->slab, slab_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&p->dev, sizeof(PoolDev) + sizeof(uint32_t) * nbuffers);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_ids, sizeof(uint32_t) * (nbuffers + 2));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->h_ids, sizeof(uint32_t) * (nbuffers + 2));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = pool_init_device(p);
+    if (e != cudaSuccess) {
+        if (p->slab) cudaFree(p->slab);
+        if (p->dev) cudaFree(p->dev);
+        if (p->d_ids) cudaFree(p->d_ids);
+        if (p->h_ids) cudaFreeHost(p->h_ids);
+        if (p->stream) cudaStreamDestroy(p->stream);
+        delete p;
+        return cuda_fail(e, "mgv_pool_create");
+    }
+    p->bufs.resize(nbuffers);
+    p->held.assign(nbuffers, 0);
+    for (uint32_t i = 0; i < nbuffers; ++i) {
+        mgv_buffer& b = p->bufs[i];
+        std::memset(&b, 0, sizeof(b));
+        for (uint32_t c = 0; c < ncols; ++c) b.cols[c] = p->slab + ((size_t)i * ncols + c) * capacity;
+        b.ncols = ncols;
+        b.capacity = capacity;
+        b.id = i;
+        b.device = ctx->device;
+    }
+    *out = p;
+    return MGV_OK;
+}
+
+mgv_status mgv_pool_destroy(mgv_pool* p) {
+    if (!p) return MGV_OK;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->stream);
+    cudaFree(p->slab);
+    cudaFree(p->dev);
+    cudaFree(p->d_ids);
+    cudaFreeHost(p->h_ids);
+    cudaStreamDestroy(p->stream);
+    delete p;
+    return MGV_OK;
+}
+
+mgv_status mgv_buffer_acquire(mgv_pool* p, uint32_t timeout_us, mgv_buffer** out) {
+    if (!p || !out) return fail(MGV_EINVAL, "NULL argument");
+    *out = nullptr;
+    std::lock_guard<std::mutex> lk(p->mu);
+    MGV_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    if (p->host_cache.empty()) {
+        uint32_t got = 0;
+        mgv_status st = MGV_OK;
+        MGV_CUDA_TRY(pool_pop_batch(p, std::min<uint32_t>(8u, p->nbuffers), timeout_us, &got, &st));
+        for (uint32_t i = 0; i < got; ++i) p->host_cache.push_back(p->h_ids[i]);
+        if (got == 0) {
+            if (st == MGV_EDRAINED) return fail(MGV_EDRAINED, "pool empty and no producer registered");
+            return fail(MGV_ETIMEDOUT, "no buffer came back before the timeout");
+        }
+    }
+    uint32_t id = p->host_cache.back();
+    p->host_cache.pop_back();
+    p->held[id] = 1;
+    p->bufs[id].rows = 0;
+    *out = &p->bufs[id];
+    return MGV_OK;
+}
+
+mgv_status mgv_buffer_release(mgv_pool* p, mgv_buffer* b) {
+    if (!p || !b) return fail(MGV_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(p->mu);
+    if (b->id >= p->nbuffers || &p->bufs[b->id] != b) return fail(MGV_EINVAL, "buffer not from this pool");
+    if (!p->held[b->id]) return fail(MGV_ESTATE, "buffer is not held");
+    p->held[b->id] = 0;
+    b->rows = 0;
+    p->host_cache.push_back(b->id);
+    if (p->host_cache.size() > 16) {
+        MGV_CUDA_TRY(cudaSetDevice(p->ctx->device));
+        const uint32_t n = 8;
+        std::vector<uint32_t> ids(p->host_cache.end() - n, p->host_cache.end());
+        p->host_cache.resize(p->host_cache.size() - n);
+        MGV_CUDA_TRY(pool_push_batch(p, ids.data(), n));
+    }
+    return MGV_OK;
+}
+
+mgv_status mgv_buffer_write(mgv_buffer* b, uint32_t col, const void* src, uint32_t rows, void* stream) {
+    if (!b || !src) return fail(MGV_EINVAL, "NULL argument");
+    if (col >= b->ncols) return fail(MGV_EINVAL, "column out of range");
+    if (rows > b->capacity) return fail(MGV_EINVAL, "rows exceed buffer capacity");
+    MGV_CUDA_TRY(cudaSetDevice(b->device));
+    if (rows) {
+        if (stream)
+            MGV_CUDA_TRY(cudaMemcpyAsync(b->cols[col], src, sizeof(int32_t) * rows, cudaMemcpyDefault,
+                                         (cudaStream_t)stream));
+        else  // blocking, as overwrite(blocking = true)
+            MGV_CUDA_TRY(cudaMemcpy(b->cols[col], src, sizeof(int32_t) * rows, cudaMemcpyDefault));
+    }
+    b->rows = rows;
+    return MGV_OK;
+}
+
+mgv_status mgv_buffer_read(const mgv_buffer* b, uint32_t col, void* dst, uint32_t rows, void* stream) {
+    if (!b || !dst) return fail(MGV_EINVAL, "NULL argument");
+    if (col >= b->ncols) return fail(MGV_EINVAL, "column out of range");
+    if (rows > b->rows) return fail(MGV_EINVAL, "rows exceed the buffer's row count");
+    MGV_CUDA_TRY(cudaSetDevice(b->device));
+    if (rows) {
+        if (stream) {
+            MGV_CUDA_TRY(cudaMemcpyAsync(dst, b->cols[col], sizeof(int32_t) * rows, cudaMemcpyDefault,
+                                         (cudaStream_t)stream));
+            MGV_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+        } else {
+            MGV_CUDA_TRY(cudaMemcpy(dst, b->cols[col], sizeof(int32_t) * rows, cudaMemcpyDefault));
+        }
+    }
+    return MGV_OK;
+}
+
+mgv_status mgv_pool_register_producer(mgv_pool* p) {
+    if (!p) return fail(MGV_EINVAL, "pool is NULL");
+    std::lock_guard<std::mutex> lk(p->mu);
+    MGV_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    MGV_CUDA_TRY(pool_add_producers(p, 1));
+    p->producers++;
+    return MGV_OK;
+}
+
+mgv_status mgv_pool_unregister_producer(mgv_pool* p) {
+    if (!p) return fail(MGV_EINVAL, "pool is NULL");
+    std::lock_guard<std::mutex> lk(p->mu);
+    if (p->producers == 0) return fail(MGV_ESTATE, "no producer registered");
+    MGV_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    MGV_CUDA_TRY(pool_add_producers(p, -1));
+    p->producers--;
+    return MGV_OK;
+}
+
+mgv_status mgv_pool_stats_get(mgv_pool* p, mgv_pool_stats* out) {
+    if (!p || !out) return fail(MGV_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(p->mu);
+    MGV_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    uint32_t avail = 0, prod = 0;
+    MGV_CUDA_TRY(pool_read_counters(p, &avail, &prod));
+    out->nbuffers = p->nbuffers;
+    out->capacity = p->capacity;
+    out->ncols = p->ncols;
+    out->available = avail;
+    out->host_cached = (uint32_t)p->host_cache.size();
+    out->producers = prod;
+    out->bytes = (uint64_t)p->nbuffers * p->ncols * p->capacity * sizeof(int32_t);
+    return MGV_OK;
+}
+
+// ---- operators -------------------------------------------------------------
+
+static mgv_op* new_op(Context* ctx, OpKind k) {
+    mgv_op* o = new (std::nothrow) mgv_op();
+    if (!o) return nullptr;
+    o->kind = k;
+    o->ctx = ctx;
+    return o;
+}
+
+static mgv_status dev_alloc(Op* o, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+    o->allocs.push_back(*p);
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_select(mgv_ctx* ctx, const mgv_select_desc* d, mgv_op* parent, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (!parent) return fail(MGV_EINVAL, "select needs a parent");
+    if (d->col >= MGV_MAX_COLS) return fail(MGV_EINVAL, "select column out of range");
+    mgv_op* o = new_op(ctx, OpKind::Select);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->sel = *d;
+    o->parent = parent;
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_aggregate(mgv_ctx* ctx, const mgv_aggregate_desc* d, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (d->sum_col_a < -1 || d->sum_col_a > MGV_MAX_COLS || d->sum_col_b < -1 || d->sum_col_b > MGV_MAX_COLS)
+        return fail(MGV_EINVAL, "sum column out of range");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_op* o = new_op(ctx, OpKind::Aggregate);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->agg = *d;
+    mgv_status st = dev_alloc(o, (void**)&o->d_acc, 2 * sizeof(unsigned long long));
+    if (st != MGV_OK) { delete o; return st; }
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_hash_build(mgv_ctx* ctx, const mgv_hash_build_desc* d, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (d->key_col >= MGV_MAX_COLS || d->payload_col < -1 || d->payload_col >= MGV_MAX_COLS)
+        return fail(MGV_EINVAL, "column out of range");
+    float lf = d->load_factor == 0.0f ? ctx->tuning.default_load_factor : d->load_factor;
+    if (!(lf > 0.0f && lf <= 0.95f)) return fail(MGV_EINVAL, "load_factor must be in (0, 0.95]");
+    const uint64_t rows = d->expected_rows ? d->expected_rows : 1;
+    const double nb = std::ceil((double)rows / (4.0 * lf));
+    if (nb >= 4294967295.0) return fail(MGV_EINVAL, "expected_rows too large");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_op* o = new_op(ctx, OpKind::HashBuild);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->hb = *d;
+    o->hb.load_factor = lf;
+    TableView& t = o->table;
+    t.nbuckets = (uint32_t)std::max(1.0, nb);
+    t.side_cap = rows;
+    o->table_bytes = (size_t)t.nbuckets * 32;
+    mgv_status st = dev_alloc(o, (void**)&t.slots, o->table_bytes);
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&t.meta, 4 * sizeof(unsigned long long));
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&t.side_pay, sizeof(int32_t) * t.side_cap);
+    if (st != MGV_OK) {
+        for (void* p : o->allocs) cudaFree(p);
+        delete o;
+        return st;
+    }
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_hash_probe(mgv_ctx* ctx, const mgv_hash_probe_desc* d, mgv_op* parent,
+                                    mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (!parent) return fail(MGV_EINVAL, "hash_probe needs a parent");
+    if (!d->build || d->build->kind != OpKind::HashBuild) return fail(MGV_EINVAL, "build must be a hash_build operator");
+    if (d->key_col >= MGV_MAX_COLS) return fail(MGV_EINVAL, "key column out of range");
+    mgv_op* o = new_op(ctx, OpKind::HashProbe);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->hp = *d;
+    o->parent = parent;
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_sink(mgv_ctx* ctx, const mgv_sink_desc* d, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (!d->pool) return fail(MGV_EINVAL, "sink needs a pool");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_op* o = new_op(ctx, OpKind::Sink);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->sk = *d;
+    o->sink_pool = d->pool;
+    uint32_t maxc = d->max_buffers ? std::min(d->max_buffers, d->pool->nbuffers) : d->pool->nbuffers;
+    SinkView& s = o->sink;
+    s.slab = d->pool->slab;
+    s.max_chunks = maxc;
+    s.capacity = d->pool->capacity;
+    s.ncols = d->pool->ncols;
+    s.pool_ncols = d->pool->ncols;
+    s.pool = d->pool->dev;
+    mgv_status st = dev_alloc(o, (void**)&s.cursor, sizeof(unsigned long long));
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&s.chain, sizeof(uint32_t) * maxc);
+    if (st != MGV_OK) {
+        for (void* p : o->allocs) cudaFree(p);
+        delete o;
+        return st;
+    }
+    *out = o;
+    return MGV_OK;
+}
+
+static mgv_status sink_return_buffers(Op* o) {
+    if (o->sink_chain.empty()) return MGV_OK;
+    Pool* p = o->sink_pool;
+    std::lock_guard<std::mutex> lk(p->mu);
+    MGV_CUDA_TRY(pool_push_batch(p, o->sink_chain.data(), (uint32_t)o->sink_chain.size()));
+    o->sink_chain.clear();
+    return MGV_OK;
+}
+
+mgv_status mgv_op_destroy(mgv_op* o) {
+    if (!o) return MGV_OK;
+    cudaSetDevice(o->ctx->device);
+    cudaStreamSynchronize(o->ctx->stream);
+    if (o->kind == OpKind::Sink) sink_return_buffers(o);
+    for (void* p : o->allocs) cudaFree(p);
+    delete o;
+    return MGV_OK;
+}
+
+// Resets one operator's device state (at_open).
+static mgv_status op_reset(Op* o, cudaStream_t s) {
+    switch (o->kind) {
+        case OpKind::Aggregate:
+            MGV_CUDA_TRY(cudaMemsetAsync(o->d_acc, 0, 2 * sizeof(unsigned long long), s));
+            o->agg_result = mgv_agg_result{0, 0};
+            break;
+        case OpKind::HashBuild:
+            MGV_CUDA_TRY(launch_fill_u64(o->table.slots, 4ull * o->table.nbuckets, kEmptySlot, s, o->ctx));
+            MGV_CUDA_TRY(cudaMemsetAsync(o->table.meta, 0, 4 * sizeof(unsigned long long), s));
+            o->unique = false;
+            break;
+        case OpKind::Sink: {
+            mgv_status st = sink_return_buffers(o);
+            if (st != MGV_OK) return st;
+            MGV_CUDA_TRY(cudaMemsetAsync(o->sink.cursor, 0, sizeof(unsigned long long), s));
+            MGV_CUDA_TRY(cudaMemsetAsync(o->sink.chain, 0xff, sizeof(uint32_t) * o->sink.max_chunks, s));
+            o->sink_rows = 0;
+            break;
+        }
+        case OpKind::HashProbe:
+            if (o->hp.build->state != OpState::Closed)
+                return fail(MGV_ESTATE, "hash_probe opened before its build side was closed");
+            break;
+        default: break;
+    }
+    return MGV_OK;
+}
+
+mgv_status mgv_op_open(mgv_op* o, void* stream) {
+    if (!o) return fail(MGV_EINVAL, "op is NULL");
+    if (o->state == OpState::Open) return fail(MGV_ESTATE, "operator already open");
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    cudaStream_t s = pick_stream(o->ctx, stream);
+    if (o->parent) {  // before_open: parents first
+        mgv_status st = mgv_op_open(static_cast<mgv_op*>(o->parent), stream);
+        if (st != MGV_OK) return st;
+    }
+    mgv_status st = op_reset(o, s);
+    if (st != MGV_OK) return st;
+    o->state = OpState::Open;
+    return MGV_OK;
+}
+
+// Reads back a terminal operator's result after its stream completed.
+static mgv_status op_finish(Op* o, cudaStream_t s) {
+    switch (o->kind) {
+        case OpKind::Aggregate: {
+            unsigned long long h[2];
+            MGV_CUDA_TRY(cudaMemcpyAsync(h, o->d_acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            o->agg_result.count = (int64_t)h[0];
+            o->agg_result.sum = (int64_t)h[1];
+            break;
+        }
+        case OpKind::HashBuild: {
+            unsigned long long m[4];
+            MGV_CUDA_TRY(cudaMemcpyAsync(m, o->table.meta, sizeof(m), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            mgv_hash_build_info& i = o->hb_info;
+            i.rows = m[2] + m[0];
+            i.nbuckets = o->table.nbuckets;
+            i.table_bytes = o->table_bytes;
+            i.reserved_key_rows = m[0];
+            i.has_duplicates = (m[3] != 0 || m[0] > 1) ? 1u : 0u;
+            o->unique = m[3] == 0;
+            break;
+        }
+        case OpKind::Sink: {
+            unsigned long long rows = 0;
+            MGV_CUDA_TRY(cudaMemcpyAsync(&rows, o->sink.cursor, sizeof(rows), cudaMemcpyDeviceToHost, s));
+            std::vector<uint32_t> chain(o->sink.max_chunks);
+            MGV_CUDA_TRY(cudaMemcpyAsync(chain.data(), o->sink.chain, sizeof(uint32_t) * chain.size(),
+                                         cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            o->sink_rows = rows;
+            o->sink_chain.clear();
+            for (uint32_t id : chain)
+                if (id < o->sink_pool->nbuffers) o->sink_chain.push_back(id);
+            break;
+        }
+        default: break;
+    }
+    return MGV_OK;
+}
+
+mgv_status mgv_op_close(mgv_op* o, void* stream) {
+    if (!o) return fail(MGV_EINVAL, "op is NULL");
+    if (o->state != OpState::Open) return fail(MGV_ESTATE, "operator is not open");
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    cudaStream_t s = pick_stream(o->ctx, stream);
+    o->state = OpState::Closed;
+    mgv_status st = MGV_OK;
+    if (!o->parent) {  // terminal: wait, check the device error word, read results
+        st = check_device(o->ctx, s);
+        mgv_status st2 = op_finish(o, s);
+        if (st == MGV_OK) st = st2;
+        return st;
+    }
+    return mgv_op_close(static_cast<mgv_op*>(o->parent), stream);  // after_close
+}
+
+mgv_status mgv_op_result(mgv_op* o, void* out, size_t bytes, size_t* needed) {
+    if (!o) return fail(MGV_EINVAL, "op is NULL");
+    if (o->state != OpState::Closed) return fail(MGV_ESTATE, "operator is not closed");
+    const void* src = nullptr;
+    size_t n = 0;
+    switch (o->kind) {
+        case OpKind::Aggregate: src = &o->agg_result; n = sizeof(o->agg_result); break;
+        case OpKind::HashBuild: src = &o->hb_info; n = sizeof(o->hb_info); break;
+        case OpKind::Sink: src = &o->sink_rows; n = sizeof(o->sink_rows); break;
+        default: return fail(MGV_EINVAL, "operator has no result");
+    }
+    if (needed) *needed = n;
+    if (!out) return MGV_OK;
+    if (bytes < n) return fail(MGV_EINVAL, "result buffer too small");
+    std::memcpy(out, src, n);
+    return MGV_OK;
+}
+
+mgv_status mgv_sink_read(mgv_op* o, uint32_t col, int32_t* dst, uint64_t max_rows, uint64_t* rows) {
+    if (!o || !dst) return fail(MGV_EINVAL, "NULL argument");
+    if (o->kind != OpKind::Sink) return fail(MGV_EINVAL, "not a sink");
+    if (o->state != OpState::Closed) return fail(MGV_ESTATE, "sink is not closed");
+    if (col >= o->sink.ncols) return fail(MGV_EINVAL, "column out of range");
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    const uint64_t cap = o->sink.capacity;
+    uint64_t total = std::min<uint64_t>(o->sink_rows, (uint64_t)o->sink_chain.size() * cap);
+    total = std::min(total, max_rows);
+    uint64_t done = 0;
+    for (size_t c = 0; c < o->sink_chain.size() && done < total; ++c) {
+        const uint64_t n = std::min<uint64_t>(cap, total - done);
+        const int32_t* src = o->sink.slab + ((size_t)o->sink_chain[c] * o->sink.pool_ncols + col) * cap;
+        MGV_CUDA_TRY(cudaMemcpyAsync(dst + done, src, n * sizeof(int32_t), cudaMemcpyDefault, o->ctx->stream));
+        done += n;
+    }
+    MGV_CUDA_TRY(cudaStreamSynchronize(o->ctx->stream));
+    if (rows) *rows = done;
+    return MGV_OK;
+}
+
+// ---- consume: match the chain to a fused kernel ---------------------------
+
+static bool all_open(Op* o) {
+    for (; o; o = o->parent)
+        if (o->state != OpState::Open) return false;
+    return true;
+}
+
+static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n,
+                               cudaStream_t s) {
+    Context* ctx = head->ctx;
+    Op* sel = nullptr;
+    Op* probe = nullptr;
+    Op* o = head;
+    if (o->kind == OpKind::Select) { sel = o; o = o->parent; }
+    if (o && o->kind == OpKind::HashProbe) { probe = o; o = o->parent; }
+    Op* term = o;
+    if (!term || term->parent) return fail(MGV_EUNSUPPORTED, "chain must be [select] [hash_probe] terminal");
+    auto col_ok = [&](int32_t c) { return c >= 0 && (uint32_t)c < ncols; };
+    if (sel && !col_ok((int32_t)sel->sel.col)) return fail(MGV_EINVAL, "select column not in input");
+    if (probe && !col_ok((int32_t)probe->hp.key_col)) return fail(MGV_EINVAL, "probe key column not in input");
+    if (n == 0) return MGV_OK;
+
+    switch (term->kind) {
+        case OpKind::Aggregate: {
+            const int32_t a = term->agg.sum_col_a, b = term->agg.sum_col_b;
+            if (!probe) {
+                if ((a != -1 && !col_ok(a)) || (b != -1 && !col_ok(b)))
+                    return fail(MGV_EINVAL, "aggregate column not in input");
+                MGV_CUDA_TRY(launch_select_agg(sel ? cols[sel->sel.col] : nullptr, sel ? sel->sel.bound : 0,
+                                               sel != nullptr, a >= 0 ? cols[a] : nullptr,
+                                               b >= 0 ? cols[b] : nullptr, n, term->d_acc, s, ctx));
+                return MGV_OK;
+            }
+            if (sel) return fail(MGV_EUNSUPPORTED, "select -> hash_probe -> aggregate is not fused yet");
+            // columns: input 0..ncols-1, build payload = ncols
+            uint32_t mode = 0;
+            const int32_t* pays = nullptr;
+            for (int32_t c : {a, b}) {
+                if (c == -1) continue;
+                if ((uint32_t)c == ncols) { mode |= 1u; continue; }
+                if (!col_ok(c)) return fail(MGV_EINVAL, "aggregate column not in input");
+                if (pays) return fail(MGV_EUNSUPPORTED, "probe aggregate sums at most one probe column");
+                pays = cols[c];
+                mode |= 2u;
+            }
+            Op* hb = probe->hp.build;
+            MGV_CUDA_TRY(launch_probe_agg(cols[probe->hp.key_col], pays, n, hb->table, hb->unique, mode,
+                                          term->d_acc, s, ctx));
+            return MGV_OK;
+        }
+        case OpKind::HashBuild: {
+            if (probe) return fail(MGV_EUNSUPPORTED, "hash_probe cannot feed hash_build");
+            const int32_t kc = (int32_t)term->hb.key_col, pc = term->hb.payload_col;
+            if (!col_ok(kc) || (pc != -1 && !col_ok(pc))) return fail(MGV_EINVAL, "build column not in input");
+            MGV_CUDA_TRY(launch_build(cols[kc], pc >= 0 ? cols[pc] : nullptr, sel ? cols[sel->sel.col] : nullptr,
+                                      sel ? sel->sel.bound : 0, sel != nullptr, n, term->table, s, ctx));
+            return MGV_OK;
+        }
+        case OpKind::Sink: {
+            ChainArgs a{};
+            for (uint32_t c = 0; c < ncols; ++c) a.cols[c] = cols[c];
+            a.ncols = ncols;
+            a.n = n;
+            a.has_sel = sel != nullptr;
+            if (sel) { a.sel_col = sel->sel.col; a.sel_bound = sel->sel.bound; }
+            a.has_probe = probe != nullptr;
+            if (probe) {
+                a.probe_col = probe->hp.key_col;
+                a.table = probe->hp.build->table;
+                a.unique = probe->hp.build->unique;
+            }
+            const uint32_t out_cols = ncols + (probe ? 1u : 0u);
+            SinkView sv = term->sink;
+            sv.ncols = std::min(out_cols, term->sink.pool_ncols);
+            MGV_CUDA_TRY(launch_chain_sink(a, sv, s, ctx));
+            return MGV_OK;
+        }
+        default: return fail(MGV_EUNSUPPORTED, "no kernel for this chain");
+    }
+}
+
+mgv_status mgv_op_consume_columns(mgv_op* o, const int32_t* const* cols, uint32_t ncols, uint64_t rows,
+                                  void* stream) {
+    if (!o || (!cols && ncols)) return fail(MGV_EINVAL, "NULL argument");
+    if (ncols > MGV_MAX_COLS) return fail(MGV_EINVAL, "too many columns");
+    if (!all_open(o)) return fail(MGV_ESTATE, "chain is not open");
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    return consume_cols(o, cols, ncols, rows, pick_stream(o->ctx, stream));
+}
+
+mgv_status mgv_op_consume(mgv_op* o, const mgv_buffer* b, void* stream) {
+    if (!o || !b) return fail(MGV_EINVAL, "NULL argument");
+    if (b->rows > b->capacity) return fail(MGV_EINVAL, "buffer rows exceed capacity");
+    return mgv_op_consume_columns(o, b->cols, b->ncols, b->rows, stream);
+}
+
+}  // extern "C"

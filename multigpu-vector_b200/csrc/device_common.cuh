@@ -1,0 +1,159 @@
+// device_common.cuh -- device-side helpers shared by every mgv kernel.
+//
+// Replaces the reference's device utilities (src/common.cuh:211-293): lane
+// and warp ids, broadcast, warp reductions.  Everything here uses the *_sync
+// warp intrinsics; the reference's legacy __shfl/__ballot rely on implicit
+// warp synchrony, which independent thread scheduling does not give.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mgv {
+
+constexpr int kWarp = 32;
+// Key value reserved as the empty-slot marker of the open-addressing hash
+// tables.  Build rows that carry this key are kept in a side list instead.
+constexpr int32_t kEmptyKey = INT32_MIN;
+constexpr unsigned long long kEmptySlot = 0x8000000080000000ull;
+
+// Device error word layout: [0] = first error code (mgv_status), [1] = detail.
+enum DevErr : uint32_t {
+    kDevOk = 0,
+    kDevTableFull = 2,      // MGV_ENOMEM
+    kDevTimeout = 3,        // MGV_ETIMEDOUT
+    kDevOverflow = 2,       // output capacity exceeded (MGV_ENOMEM)
+};
+
+__device__ __forceinline__ uint32_t lane_id() {
+    uint32_t l;
+    asm("mov.u32 %0, %%laneid;" : "=r"(l));
+    return l;
+}
+
+// MurmurHash3 32-bit finaliser; the reference's hashMurmur
+// (src/operators/hashjoin.cu:4-11).
+__host__ __device__ __forceinline__ uint32_t murmur32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// Bucket of a key in a table of nbuckets buckets: multiply-shift range
+// reduction of the murmur hash, so nbuckets need not be a power of two.
+__device__ __forceinline__ uint32_t bucket_of(int32_t key, uint32_t nbuckets) {
+    return __umulhi(murmur32((uint32_t)key), nbuckets);
+}
+
+__device__ __forceinline__ void set_error(uint32_t* err, uint32_t code, uint32_t detail) {
+    if (atomicCAS(err, 0u, code) == 0u) atomicExch(err + 1, detail);
+}
+
+// 32 bytes of a streamed column: no L1 allocation and first-out in L2, so
+// that streamed input does not push resident hash tables out of L2.
+__device__ __forceinline__ void ld_stream8(const int32_t* p, int32_t (&v)[8]) {
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.L2::evict_first.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+        : "l"(p));
+}
+
+// One 32-byte hash bucket (4 slots of {key, payload}), read-only during a
+// probe: kept in L2 with evict_last priority, not allocated in L1.
+__device__ __forceinline__ void ld_bucket(const unsigned long long* p, uint32_t (&w)[8]) {
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.L2::evict_last.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+        : "l"(p));
+}
+
+// The same bucket read coherently at gpu scope while it is being filled.
+__device__ __forceinline__ void ld_bucket_relaxed(const unsigned long long* p, unsigned long long (&s)[4]) {
+    asm volatile("ld.relaxed.gpu.global.v4.b64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(s[0]), "=l"(s[1]), "=l"(s[2]), "=l"(s[3])
+                 : "l"(p));
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of two u64 values, then one atomicAdd each into acc[0..1].
+// Two's-complement addition makes this exact for int64 sums too.
+template <int BLOCK>
+__device__ __forceinline__ void block_accumulate2(unsigned long long a, unsigned long long b,
+                                                  unsigned long long* acc) {
+    __shared__ unsigned long long red[2][BLOCK / kWarp];
+    a = warp_sum_u64(a);
+    b = warp_sum_u64(b);
+    const int w = threadIdx.x / kWarp;
+    if (lane_id() == 0) { red[0][w] = a; red[1][w] = b; }
+    __syncthreads();
+    if (threadIdx.x < kWarp) {
+        unsigned long long x = threadIdx.x < BLOCK / kWarp ? red[0][threadIdx.x] : 0ull;
+        unsigned long long y = threadIdx.x < BLOCK / kWarp ? red[1][threadIdx.x] : 0ull;
+        x = warp_sum_u64(x);
+        y = warp_sum_u64(y);
+        if (threadIdx.x == 0) {
+            if (x) atomicAdd(acc + 0, x);
+            if (y) atomicAdd(acc + 1, y);
+        }
+    }
+}
+
+}  // namespace mgv
+
+namespace mgv {
+
+// ---- mbarrier + bulk async copy (TMA engine, non-tensor form) -------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bulk copy global -> shared, completion counted on `bar` (bytes % 16 == 0,
+// both addresses 16-byte aligned).  Never multicast.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`; false if it ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t max_tries) {
+    for (uint32_t i = 0; i < max_tries; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+}  // namespace mgv

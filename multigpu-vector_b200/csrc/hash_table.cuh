@@ -1,0 +1,100 @@
+// hash_table.cuh -- device logic of the open-addressing join table.
+//
+// Layout: nbuckets buckets of 32 bytes (one L2 sector), 4 slots each; a
+// slot is a 64-bit {key (low word), payload (high word)}.  The key
+// INT32_MIN marks an empty slot; build rows with that key go to a side
+// list.  A key's run starts at bucket_of(key) and continues linearly;
+// slots of a run are claimed in order, so a lookup may stop at the first
+// empty slot (and, for tables without duplicate keys, at the first match).
+//
+// Replaces the reference's chained table: first[2^L] + next[2 * max]
+// (src/operators/hashjoin.cu:40-75), whose probe walks dependent pointers.
+#pragma once
+
+#include "device_common.cuh"
+#include "mgv_internal.h"
+
+namespace mgv {
+
+__device__ __forceinline__ void table_insert(const TableView& t, int32_t key, int32_t pay,
+                                             uint32_t* err, bool& dup, bool& ok) {
+    ok = false;
+    if (key == kEmptyKey) {
+        unsigned long long i = atomicAdd(t.meta + 0, 1ull);
+        atomicAdd(t.meta + 1, (unsigned long long)(long long)pay);
+        if (i < t.side_cap) t.side_pay[i] = pay;
+        else set_error(err, kDevTableFull, 1);
+        return;
+    }
+    const unsigned long long v = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
+    uint32_t b = bucket_of(key, t.nbuckets);
+    for (uint32_t it = 0; it < t.nbuckets; ++it) {
+        unsigned long long s[4];
+        ld_bucket_relaxed(t.slots + 4ull * b, s);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            unsigned long long cur = s[j];
+            if ((int32_t)(uint32_t)cur == kEmptyKey) {
+                unsigned long long old = atomicCAS(t.slots + 4ull * b + j, kEmptySlot, v);
+                if (old == kEmptySlot) {
+                    ok = true;
+                    return;
+                }
+                cur = old;
+            }
+            if ((int32_t)(uint32_t)cur == key) dup = true;
+        }
+        b = (b + 1 == t.nbuckets) ? 0u : b + 1;
+    }
+    set_error(err, kDevTableFull, 2);
+}
+
+// Matches of `key` inside one bucket w[0..7] = k0 p0 k1 p1 k2 p2 k3 p3.
+// more = the probe must continue to the next bucket.
+template <bool UNIQUE>
+__device__ __forceinline__ void match_bucket(const uint32_t (&w)[8], int32_t key, uint32_t& mc,
+                                             long long& ms, bool& more) {
+    const uint32_t k = (uint32_t)key;
+    const bool m0 = w[0] == k, m1 = w[2] == k, m2 = w[4] == k, m3 = w[6] == k;
+    const bool full = w[6] != (uint32_t)kEmptyKey;
+    if (UNIQUE) {
+        const bool f = m0 | m1 | m2 | m3;
+        mc = f;
+        ms = f ? (long long)(int32_t)(m0 ? w[1] : m1 ? w[3] : m2 ? w[5] : w[7]) : 0ll;
+        more = !f && full;
+    } else {
+        mc = (uint32_t)m0 + m1 + m2 + m3;
+        ms = (m0 ? (long long)(int32_t)w[1] : 0ll) + (m1 ? (long long)(int32_t)w[3] : 0ll) +
+             (m2 ? (long long)(int32_t)w[5] : 0ll) + (m3 ? (long long)(int32_t)w[7] : 0ll);
+        more = full;
+    }
+}
+
+// Continuation past a full home bucket (rare at the default load factor).
+// Returns {matches, payload sum}; kept out of line so the common path of
+// the probe loop stays small.
+struct Matches {
+    unsigned long long sum;
+    uint32_t count;
+};
+
+template <bool UNIQUE>
+__device__ __forceinline__ Matches probe_rest(const unsigned long long* __restrict__ slots,
+                                           uint32_t nbuckets, int32_t key, uint32_t b) {
+    Matches r{0ull, 0u};
+    for (uint32_t it = 1; it < nbuckets; ++it) {
+        b = (b + 1 == nbuckets) ? 0u : b + 1;
+        uint32_t w[8];
+        ld_bucket(slots + 4ull * b, w);
+        uint32_t c;
+        long long s;
+        bool more;
+        match_bucket<UNIQUE>(w, key, c, s, more);
+        r.count += c;
+        r.sum += (unsigned long long)s;
+        if (!more) break;
+    }
+    return r;
+}
+
+}  // namespace mgv

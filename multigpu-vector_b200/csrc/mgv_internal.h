@@ -1,0 +1,184 @@
+// mgv_internal.h -- host-side objects behind the C ABI and the kernel
+// launchers they call.  Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mgv.h"
+
+namespace mgv {
+
+// ---- error reporting ---------------------------------------------------
+
+void set_last_error(const std::string& msg);
+mgv_status fail(mgv_status s, const std::string& msg);
+mgv_status cuda_fail(cudaError_t e, const char* what);
+
+#define MGV_CUDA_TRY(expr)                                    \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return ::mgv::cuda_fail(e_, #expr); \
+    } while (0)
+
+// ---- device views passed to kernels by value ----------------------------
+
+// Open-addressing join table: nbuckets buckets of 4 slots, each slot a
+// 64-bit {key (low word), payload (high word)}; 32-byte aligned buckets.
+struct TableView {
+    unsigned long long* slots;
+    uint32_t nbuckets;
+    uint32_t pad;
+    // Rows whose key is the reserved empty marker INT32_MIN:
+    // meta[0] = their count, meta[1] = their payload sum, meta[2] = rows
+    // inserted into the table, meta[3] = duplicate-key flag.
+    unsigned long long* meta;
+    int32_t* side_pay;      // payloads of those rows (for emitting matches)
+    uint64_t side_cap;
+};
+
+// Output rows appended to a chain of pool buffers.
+struct SinkView {
+    int32_t* slab;              // pool slab base
+    unsigned long long* cursor; // rows reserved so far
+    uint32_t* chain;            // buffer id per chunk, 0xffffffff = not yet taken
+    uint32_t max_chunks;
+    uint32_t capacity;          // rows per buffer
+    uint32_t ncols;             // columns written
+    uint32_t pool_ncols;
+    struct PoolDev* pool;       // device free stack for swap-on-full
+};
+
+// Device free stack of a pool (tagged Treiber stack of buffer ids).
+struct PoolDev {
+    unsigned long long head;    // low 32 bits: top id (0xffffffff = empty), high: tag
+    uint32_t available;
+    uint32_t producers;
+    uint32_t nbuffers;
+    uint32_t pad;
+    uint32_t next[1];           // nbuffers entries follow
+};
+
+constexpr uint32_t kNil = 0xffffffffu;
+
+// ---- host objects --------------------------------------------------------
+
+struct Context;
+
+struct Pool {
+    Context* ctx = nullptr;
+    uint32_t nbuffers = 0, capacity = 0, ncols = 0;
+    int32_t* slab = nullptr;
+    PoolDev* dev = nullptr;         // device free stack
+    uint32_t* d_ids = nullptr;      // device scratch for host batch ops
+    uint32_t* h_ids = nullptr;      // pinned mirror
+    cudaStream_t stream = nullptr;  // the pool's own stream (release_streams)
+    std::mutex mu;
+    std::vector<uint32_t> host_cache;   // ids cached on the host side
+    std::vector<mgv_buffer> bufs;       // descriptors, indexed by id
+    std::vector<uint8_t> held;          // 1 = handed out to the caller
+    uint32_t producers = 0;
+};
+
+struct Context {
+    int device = 0;
+    cudaDeviceProp prop{};
+    cudaStream_t stream = nullptr;
+    uint32_t* d_err = nullptr;      // device error word [code, detail]
+    std::atomic<uint64_t> launches{0};
+    mgv_tuning tuning{0u, 4u, 4u, 0u, 0.5f, {0u, 0u, 0u}};
+    std::mutex mu;
+};
+
+enum class OpKind { Select, Aggregate, HashBuild, HashProbe, Sink };
+enum class OpState { Created, Open, Closed };
+
+struct Op {
+    OpKind kind;
+    Context* ctx = nullptr;
+    Op* parent = nullptr;
+    OpState state = OpState::Created;
+    // select
+    mgv_select_desc sel{};
+    // aggregate
+    mgv_aggregate_desc agg{};
+    unsigned long long* d_acc = nullptr;    // [count, sum]
+    mgv_agg_result agg_result{};
+    // hash build
+    mgv_hash_build_desc hb{};
+    TableView table{};
+    size_t table_bytes = 0;
+    mgv_hash_build_info hb_info{};
+    bool unique = false;
+    // hash probe
+    mgv_hash_probe_desc hp{};
+    // sink
+    mgv_sink_desc sk{};
+    Pool* sink_pool = nullptr;
+    SinkView sink{};
+    uint64_t sink_rows = 0;
+    std::vector<uint32_t> sink_chain;
+    // device allocations owned by this op
+    std::vector<void*> allocs;
+};
+
+// ---- kernel launchers (kernels.cu, pool.cu) -----------------------------
+
+struct LaunchCfg {
+    int grid;
+    int block;
+};
+
+int occupancy_grid(const void* kernel, int block, size_t smem, const Context* ctx);
+
+cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long long v, cudaStream_t s,
+                            Context* ctx);
+cudaError_t launch_select_agg(const int32_t* filt, int32_t bound, bool has_sel, const int32_t* a,
+                              const int32_t* b, uint64_t n, unsigned long long* acc, cudaStream_t s,
+                              Context* ctx);
+cudaError_t launch_build(const int32_t* keys, const int32_t* pays, const int32_t* filt,
+                         int32_t bound, bool has_sel, uint64_t n, const TableView& t,
+                         cudaStream_t s, Context* ctx);
+// sum_mode bit 0: add build payload, bit 1: add probe payload column.
+cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
+                                    bool unique, uint32_t sum_mode, unsigned long long* acc, cudaStream_t s,
+                                    Context* ctx);
+cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t n,
+                             const TableView& t, bool unique, uint32_t sum_mode,
+                             unsigned long long* acc, cudaStream_t s, Context* ctx);
+// Generic fused chain: [select] -> [probe] -> sink.
+struct ChainArgs {
+    const int32_t* cols[MGV_MAX_COLS];
+    uint32_t ncols;
+    uint64_t n;
+    bool has_sel;
+    uint32_t sel_col;
+    int32_t sel_bound;
+    bool has_probe;
+    uint32_t probe_col;
+    TableView table;
+    bool unique;
+};
+cudaError_t launch_chain_sink(const ChainArgs& a, const SinkView& sink, cudaStream_t s,
+                              Context* ctx);
+
+// pool.cu
+cudaError_t pool_init_device(Pool* p);
+// Pops up to `want` ids into p->h_ids (sync); returns the count taken or
+// reports drained / timeout through *status.
+cudaError_t pool_pop_batch(Pool* p, uint32_t want, uint32_t timeout_us, uint32_t* got,
+                           mgv_status* status);
+cudaError_t pool_push_batch(Pool* p, const uint32_t* ids, uint32_t n);
+cudaError_t pool_read_counters(Pool* p, uint32_t* available, uint32_t* producers);
+cudaError_t pool_add_producers(Pool* p, int delta);
+
+}  // namespace mgv
+
+struct mgv_ctx : mgv::Context {};
+struct mgv_pool : mgv::Pool {};
+struct mgv_op : mgv::Op {};

@@ -1,0 +1,350 @@
+// probe_staged.cu -- hash probe -> aggregate, warp-specialised.
+//
+// A random 32-byte bucket read costs one L1TEX request, and an SM retires
+// about one such request per clock; the probe is bound by that rate, not by
+// HBM.  The kernel therefore spends the SM's request slots on bucket reads
+// only:
+//
+//   * a producer warp streams the probe columns (key, payload) into an
+//     S-stage shared-memory ring with cp.async.bulk (TMA engine), one
+//     mbarrier pair (full / empty) per stage, so column streaming issues no
+//     L1 requests and runs S tiles ahead;
+//   * 8 consumer warps take R rows per lane from a landed stage, release the
+//     stage, and issue R independent bucket loads;
+//   * a probe whose run continues past a full bucket (about 5% at load
+//     factor 0.5) is not chased on the spot, which would add a dependent L2
+//     round trip to nearly every warp iteration; it is appended to the
+//     warp's continuation queue in shared memory, and once 32 are queued
+//     each lane takes one and issues its load together with the next
+//     round's home-bucket loads.  Before each round the warp drains until
+//     the round cannot overflow the queue, so nothing is ever dropped.
+//
+// Every mbarrier wait is bounded; a wait that runs out sets the context's
+// error word and the kernel ends (after a bounded drain of the copies in
+// flight), so the host sees MGV_ETIMEDOUT instead of a hung GPU.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "hash_table.cuh"
+#include "mgv_internal.h"
+
+namespace mgv {
+
+namespace {
+
+constexpr int kConsumerWarps = 8;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
+// continuation queue entries per consumer warp: room for two full rounds
+template <int R>
+constexpr int queue_len() { return 32 * (R + 1) <= 128 ? 256 : 512; }
+constexpr uint32_t kWaitTries = 1u << 24;
+
+struct Acc {
+    unsigned long long cnt, sum;
+};
+
+// Per-warp continuation queue (ring) in shared memory.
+struct ContQueue {
+    int32_t* key;
+    int32_t* pay;
+    uint32_t* bucket;
+    uint32_t head;   // warp-uniform
+    uint32_t count;  // warp-uniform
+};
+
+__device__ __forceinline__ uint32_t next_bucket(uint32_t b, uint32_t nb) { return (b + 1 == nb) ? 0u : b + 1; }
+
+// Fold one bucket's matches for (key, pay); returns whether the run goes on.
+template <bool UNIQUE, bool ADD_BP, bool ADD_PP>
+__device__ __forceinline__ bool fold(const uint32_t (&w)[8], int32_t key, int32_t pay, Acc& a) {
+    uint32_t mc;
+    long long ms;
+    bool more;
+    match_bucket<UNIQUE>(w, key, mc, ms, more);
+    a.cnt += mc;
+    long long add = 0;
+    if (ADD_BP) add += ms;
+    if (ADD_PP) add += (long long)mc * pay;
+    a.sum += (unsigned long long)add;
+    return more;
+}
+
+// Warp-wide append of the lanes with `push` set.  Callers keep the queue
+// below Q - 32 * (R + 1) before a round, so an append always fits.
+template <int Q>
+__device__ __forceinline__ void enqueue(ContQueue& q, bool push, int32_t key, int32_t pay, uint32_t b) {
+    const unsigned m = __ballot_sync(0xffffffffu, push);
+    if (m == 0) return;
+    const uint32_t lane = lane_id();
+    if (push) {
+        const uint32_t idx = (q.head + q.count + __popc(m & ((1u << lane) - 1u))) & (Q - 1);
+        q.key[idx] = key;
+        q.pay[idx] = pay;
+        q.bucket[idx] = b;
+    }
+    q.count += __popc(m);
+    __syncwarp();
+}
+
+// One round for a warp: R rows per lane (valid bits in `valid`) plus, when
+// the queue holds a batch (or `drain`), one continuation per lane.
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+__device__ __forceinline__ void round(const int32_t (&k)[R], const int32_t (&p)[R], uint32_t valid, ContQueue& q,
+                                      bool drain, const TableView& t, Acc& a) {
+    const uint32_t lane = lane_id();
+    // take a continuation batch
+    int32_t ck = 0, cp = 0;
+    uint32_t cb = 0;
+    bool has_c = false;
+    if (q.count >= 32 || (drain && q.count > 0)) {
+        const uint32_t m = q.count < 32 ? q.count : 32;
+        if (lane < m) {
+            const uint32_t idx = (q.head + lane) & (Q - 1);
+            ck = q.key[idx];
+            cp = q.pay[idx];
+            cb = q.bucket[idx];
+            has_c = true;
+        }
+        q.head = (q.head + m) & (Q - 1);
+        q.count -= m;
+        __syncwarp();
+    }
+    // issue every load of the round before looking at any of them
+    uint32_t hb[R];
+    uint32_t w[R][8];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        hb[r] = bucket_of(k[r], t.nbuckets);
+        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * hb[r], w[r]);
+    }
+    uint32_t wc[8];
+    if (has_c) ld_bucket(t.slots + 4ull * cb, wc);
+
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        bool more = false;
+        if ((valid >> r) & 1u) {
+            if (k[r] == kEmptyKey) {
+                const unsigned long long c = t.meta[0];
+                a.cnt += c;
+                long long add = 0;
+                if (ADD_BP) add += (long long)t.meta[1];
+                if (ADD_PP) add += (long long)c * p[r];
+                a.sum += (unsigned long long)add;
+            } else {
+                more = fold<UNIQUE, ADD_BP, ADD_PP>(w[r], k[r], p[r], a);
+            }
+        }
+        enqueue<Q>(q, more, k[r], p[r], next_bucket(hb[r], t.nbuckets));
+    }
+    bool cmore = false;
+    if (has_c) cmore = fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a);
+    enqueue<Q>(q, cmore, ck, cp, next_bucket(cb, t.nbuckets));
+}
+
+// Continuation-only rounds until a full round can no longer overflow the
+// queue.  They never grow it, and every run ends, so this terminates.
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+__device__ __forceinline__ void make_room(ContQueue& q, const TableView& t, Acc& a, uint32_t limit) {
+    int32_t z[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) z[r] = 0;
+    for (uint32_t guard = 0; q.count > limit && guard < (1u << 24); ++guard)
+        round<R, Q, UNIQUE, ADD_BP, ADD_PP>(z, z, 0u, q, true, t, a);
+}
+
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+__global__ void __launch_bounds__(kThreads, MB)
+    k_probe_agg_ws(const int32_t* __restrict__ keys, const int32_t* __restrict__ pays, uint64_t n, TableView t,
+                   unsigned long long* acc, uint32_t* err) {
+    constexpr int T = kConsumerWarps * 32 * R;  // rows per tile
+    constexpr int Q = queue_len<R>();
+    constexpr uint32_t kRoomLimit = (uint32_t)(Q - 32 * (R + 1));
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    int32_t* sk = reinterpret_cast<int32_t*>(smem_raw);
+    int32_t* sp = sk + S * T;
+    int32_t* qbase = sp + (ADD_PP ? S * T : 0);
+    uint64_t* full = reinterpret_cast<uint64_t*>(qbase + 3 * kConsumerWarps * Q);
+    uint64_t* empty = full + S;
+
+    const uint64_t nfull = n / T;
+    const uint64_t my_tiles = nfull > blockIdx.x ? (nfull - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const uint32_t tile_bytes = (uint32_t)T * sizeof(int32_t);
+    const int warp = threadIdx.x / 32;
+    const uint32_t lane = lane_id();
+    const uint32_t zero = (uint32_t)(n >> 63);  // 0 for every real row count
+
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    Acc a{0ull, 0ull};
+    if (warp == kConsumerWarps) {
+        // ---- producer warp: keep S tiles of the probe columns in flight ----
+        if (lane == 0) {
+            uint64_t i = 0;
+            for (; i < my_tiles; ++i) {
+                const int s = (int)(i % S);
+                if (i >= (uint64_t)S &&
+                    !mbar_wait_bounded(&empty[s], (uint32_t)(((i / S) - 1) & 1), kWaitTries)) {
+                    set_error(err, kDevTimeout, 11);
+                    break;
+                }
+                const uint64_t tile = blockIdx.x + i * gridDim.x;
+                mbar_expect_tx(&full[s], ADD_PP ? 2 * tile_bytes : tile_bytes);
+                bulk_g2s(sk + s * T, keys + tile * T, tile_bytes, &full[s]);
+                if (ADD_PP) bulk_g2s(sp + s * T, pays + tile * T, tile_bytes, &full[s]);
+            }
+            // let every copy issued land before the CTA can exit
+            const uint64_t lo = i > (uint64_t)S ? i - S : 0;
+            for (uint64_t j = lo; j < i; ++j) mbar_wait_bounded(&full[j % S], (uint32_t)((j / S) & 1), kWaitTries);
+        }
+    } else {
+        // ---- consumer warps ----
+        ContQueue q;
+        q.key = qbase + warp * Q;
+        q.pay = qbase + (kConsumerWarps + warp) * Q;
+        q.bucket = reinterpret_cast<uint32_t*>(qbase + (2 * kConsumerWarps + warp) * Q);
+        q.head = 0;
+        q.count = 0;
+        const int row0 = (warp * 32 + (int)lane) * R;
+        bool ok = true;
+        for (uint64_t i = 0; i < my_tiles; ++i) {
+            const int s = (int)(i % S);
+            if (!mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1), kWaitTries)) {
+                ok = false;
+            }
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) set_error(err, kDevTimeout, 12);
+                break;
+            }
+            int32_t k[R], p[R];
+#pragma unroll
+            for (int r = 0; r < R; r += 4) {
+                const int4 v = *reinterpret_cast<const int4*>(sk + s * T + row0 + r);
+                k[r] = v.x; k[r + 1] = v.y; k[r + 2] = v.z; k[r + 3] = v.w;
+                if (ADD_PP) {
+                    const int4 u = *reinterpret_cast<const int4*>(sp + s * T + row0 + r);
+                    p[r] = u.x; p[r + 1] = u.y; p[r + 2] = u.z; p[r + 3] = u.w;
+                } else {
+                    p[r] = p[r + 1] = p[r + 2] = p[r + 3] = 0;
+                }
+            }
+            // Release the stage only once every lane's reads of it have
+            // landed: fold the loaded values, combine them across the warp
+            // (the reduction waits for each lane's loads), order the reads
+            // before the async-proxy (TMA) refill, and make the arrive's
+            // address depend on the combined value (through a run-time zero
+            // the compiler cannot fold away).
+            uint32_t dep = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) dep ^= (uint32_t)k[r] ^ (uint32_t)p[r];
+            const uint32_t wdep = __reduce_or_sync(0xffffffffu, dep);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (lane == 0) {
+                const uint32_t addr = smem_u32(&empty[s]) + ((wdep & zero) << 3);
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+            }
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(k, p, (1u << R) - 1u, q, false, t, a);
+        }
+        if (ok && blockIdx.x == gridDim.x - 1) {
+            // rows of the last partial tile, straight from global memory
+            const uint64_t base = nfull * T + (uint64_t)row0;
+            int32_t k[R], p[R];
+            uint32_t valid = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const bool in = base + r < n;
+                k[r] = in ? keys[base + r] : 0;
+                p[r] = (in && ADD_PP) ? pays[base + r] : 0;
+                valid |= (uint32_t)in << r;
+            }
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(k, p, valid, q, false, t, a);
+        }
+        // drain the continuation queue
+        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, 0u);
+    }
+    block_accumulate2<kThreads>(a.cnt, a.sum, acc);
+}
+
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
+                     unsigned long long* acc, int ctas_per_sm, cudaStream_t s, Context* ctx) {
+    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP>;
+    constexpr int T = kConsumerWarps * 32 * R;
+    const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
+                        (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) + 2 * S * sizeof(uint64_t);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+    uint64_t grid = (uint64_t)per_sm * ctx->prop.multiProcessorCount;
+    const uint64_t nfull = n / T;
+    if (grid > nfull) grid = nfull ? nfull : 1;
+    k<<<(int)grid, kThreads, smem, s>>>(keys, pays, n, t, acc, ctx->d_err);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+template <int R, int S, int MB, bool UNIQUE>
+cudaError_t launch_mode(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t, uint32_t mode,
+                        unsigned long long* acc, int ctas, cudaStream_t s, Context* ctx) {
+    switch (mode) {
+        case 0: return launch_v<R, S, MB, UNIQUE, false, false>(keys, pays, n, t, acc, ctas, s, ctx);
+        case 1: return launch_v<R, S, MB, UNIQUE, true, false>(keys, pays, n, t, acc, ctas, s, ctx);
+        case 2: return launch_v<R, S, MB, UNIQUE, false, true>(keys, pays, n, t, acc, ctas, s, ctx);
+        default: return launch_v<R, S, MB, UNIQUE, true, true>(keys, pays, n, t, acc, ctas, s, ctx);
+    }
+}
+
+}  // namespace
+
+// Returns cudaErrorNotSupported when this kernel does not apply (columns
+// not 16-byte aligned); the caller then uses the register-prefetch kernel.
+cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
+                                    bool unique, uint32_t sum_mode, unsigned long long* acc, cudaStream_t s,
+                                    Context* ctx) {
+    if (((uintptr_t)keys & 15u) || ((uintptr_t)pays & 15u)) return cudaErrorNotSupported;
+    const uint32_t mode = (sum_mode & 1u) | ((sum_mode & 2u) && pays ? 2u : 0u);
+    const mgv_tuning& tu = ctx->tuning;
+    const int ctas = (int)tu.probe_ctas_per_sm;
+    const int st = tu.probe_stages <= 2 ? 2 : tu.probe_stages <= 4 ? 4 : 6;
+    // Register budgets without spills on the unique-key path: R = 4 at 2 or
+    // 3 CTAs per SM (the latter when probe_ctas_per_sm asks for 3), R = 8 at 1.
+#define MGV_WS(RR, SS, MBB)                                                                        \
+    return unique ? launch_mode<RR, SS, MBB, true>(keys, pays, n, t, mode, acc, ctas, s, ctx)     \
+                  : launch_mode<RR, SS, MBB, false>(keys, pays, n, t, mode, acc, ctas, s, ctx)
+    if (tu.probe_rows_per_thread == 8) {
+        switch (st) {
+            case 2: MGV_WS(8, 2, 1);
+            case 4: MGV_WS(8, 4, 1);
+            default: MGV_WS(8, 6, 1);
+        }
+    }
+    if (ctas == 3) {
+        switch (st) {
+            case 2: MGV_WS(4, 2, 3);
+            case 4: MGV_WS(4, 4, 3);
+            default: MGV_WS(4, 6, 3);
+        }
+    }
+    switch (st) {
+        case 2: MGV_WS(4, 2, 2);
+        case 4: MGV_WS(4, 4, 2);
+        default: MGV_WS(4, 6, 2);
+    }
+#undef MGV_WS
+}
+
+}  // namespace mgv

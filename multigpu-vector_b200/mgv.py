@@ -1,0 +1,397 @@
+"""ctypes binding of libmgv (include/mgv.h) and the reference-style plans.
+
+The library is the product: every operator runs as a CUDA kernel for
+sm_100a inside libmgv.so.  This module only binds the C ABI and builds the
+operator chains the reference's drivers build (``create_sum_select_pipeline``
+and ``create_count_join_1G_pipeline`` in src/main9.cu:202-367), so that callers
+and tests read like the reference's own plans.  There is no CPU fallback:
+importing this module without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from ctypes import POINTER, byref, c_char, c_double, c_float, c_int, c_int32, c_int64, c_size_t
+from ctypes import c_uint32, c_uint64, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmgv.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "mgv.h")
+
+MAX_COLS = 8
+# Rows per pool buffer by default (DEFAULT_BUFF_CAP, src/common.cuh:8-10).
+DEFAULT_BUFFER_ROWS = 4 * 1024 * 1024
+
+# mgv_status
+OK, EINVAL, ENOMEM, ETIMEDOUT, ECUDA, EDEVICE, ESTATE, EDRAINED, EUNSUPPORTED = range(9)
+STATUS_NAMES = {
+    OK: "MGV_OK", EINVAL: "MGV_EINVAL", ENOMEM: "MGV_ENOMEM", ETIMEDOUT: "MGV_ETIMEDOUT",
+    ECUDA: "MGV_ECUDA", EDEVICE: "MGV_EDEVICE", ESTATE: "MGV_ESTATE", EDRAINED: "MGV_EDRAINED",
+    EUNSUPPORTED: "MGV_EUNSUPPORTED",
+}
+
+
+class MgvError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {detail}")
+        self.status = status
+
+
+class Buffer(ctypes.Structure):
+    _fields_ = [("cols", c_void_p * MAX_COLS), ("ncols", c_uint32), ("rows", c_uint32),
+                ("capacity", c_uint32), ("id", c_uint32), ("device", c_int32), ("reserved", c_uint32)]
+
+
+class CtxInfo(ctypes.Structure):
+    _fields_ = [("device", c_int32), ("sm_count", c_int32), ("l2_bytes", c_uint64),
+                ("hbm_bytes", c_uint64), ("cc_major", c_int32), ("cc_minor", c_int32),
+                ("name", c_char * 64)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("probe_kernel", c_uint32), ("probe_rows_per_thread", c_uint32), ("probe_stages", c_uint32),
+                ("probe_ctas_per_sm", c_uint32), ("default_load_factor", c_float), ("reserved", c_uint32 * 3)]
+
+
+class PoolStats(ctypes.Structure):
+    _fields_ = [("nbuffers", c_uint32), ("capacity", c_uint32), ("ncols", c_uint32),
+                ("available", c_uint32), ("host_cached", c_uint32), ("producers", c_uint32),
+                ("bytes", c_uint64)]
+
+
+class SelectDesc(ctypes.Structure):
+    _fields_ = [("col", c_uint32), ("bound", c_int32)]
+
+
+class AggregateDesc(ctypes.Structure):
+    _fields_ = [("sum_col_a", c_int32), ("sum_col_b", c_int32)]
+
+
+class AggResult(ctypes.Structure):
+    _fields_ = [("count", c_int64), ("sum", c_int64)]
+
+
+class HashBuildDesc(ctypes.Structure):
+    _fields_ = [("key_col", c_uint32), ("payload_col", c_int32), ("expected_rows", c_uint64),
+                ("load_factor", c_float), ("reserved", c_uint32)]
+
+
+class HashBuildInfo(ctypes.Structure):
+    _fields_ = [("rows", c_uint64), ("nbuckets", c_uint64), ("table_bytes", c_uint64),
+                ("reserved_key_rows", c_uint64), ("has_duplicates", c_uint32), ("reserved", c_uint32)]
+
+
+class HashProbeDesc(ctypes.Structure):
+    _fields_ = [("key_col", c_uint32), ("reserved", c_uint32), ("build", c_void_p)]
+
+
+class SinkDesc(ctypes.Structure):
+    _fields_ = [("pool", c_void_p), ("max_buffers", c_uint32), ("reserved", c_uint32)]
+
+
+_lib = None
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of the functions include/mgv.h declares."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mgv_[a-z0-9_]+)\s*\(", text)))
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libmgv.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libmgv.so is not built ({path}); run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    st = c_int
+    sigs = {
+        "mgv_status_string": (ctypes.c_char_p, [c_int]),
+        "mgv_last_error_string": (ctypes.c_char_p, []),
+        "mgv_ctx_create": (st, [c_int, POINTER(c_void_p)]),
+        "mgv_ctx_destroy": (st, [c_void_p]),
+        "mgv_ctx_info_get": (st, [c_void_p, POINTER(CtxInfo)]),
+        "mgv_ctx_sync": (st, [c_void_p, c_void_p]),
+        "mgv_ctx_launches": (c_uint64, [c_void_p]),
+        "mgv_ctx_set_tuning": (st, [c_void_p, POINTER(Tuning)]),
+        "mgv_ctx_get_tuning": (st, [c_void_p, POINTER(Tuning)]),
+        "mgv_pool_create": (st, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(c_void_p)]),
+        "mgv_pool_destroy": (st, [c_void_p]),
+        "mgv_buffer_acquire": (st, [c_void_p, c_uint32, POINTER(POINTER(Buffer))]),
+        "mgv_buffer_release": (st, [c_void_p, POINTER(Buffer)]),
+        "mgv_buffer_write": (st, [POINTER(Buffer), c_uint32, c_void_p, c_uint32, c_void_p]),
+        "mgv_buffer_read": (st, [POINTER(Buffer), c_uint32, c_void_p, c_uint32, c_void_p]),
+        "mgv_pool_register_producer": (st, [c_void_p]),
+        "mgv_pool_unregister_producer": (st, [c_void_p]),
+        "mgv_pool_stats_get": (st, [c_void_p, POINTER(PoolStats)]),
+        "mgv_op_create_select": (st, [c_void_p, POINTER(SelectDesc), c_void_p, POINTER(c_void_p)]),
+        "mgv_op_create_aggregate": (st, [c_void_p, POINTER(AggregateDesc), POINTER(c_void_p)]),
+        "mgv_op_create_hash_build": (st, [c_void_p, POINTER(HashBuildDesc), POINTER(c_void_p)]),
+        "mgv_op_create_hash_probe": (st, [c_void_p, POINTER(HashProbeDesc), c_void_p, POINTER(c_void_p)]),
+        "mgv_op_create_sink": (st, [c_void_p, POINTER(SinkDesc), POINTER(c_void_p)]),
+        "mgv_op_destroy": (st, [c_void_p]),
+        "mgv_op_open": (st, [c_void_p, c_void_p]),
+        "mgv_op_consume": (st, [c_void_p, POINTER(Buffer), c_void_p]),
+        "mgv_op_consume_columns": (st, [c_void_p, POINTER(c_void_p), c_uint32, c_uint64, c_void_p]),
+        "mgv_op_close": (st, [c_void_p, c_void_p]),
+        "mgv_op_result": (st, [c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]),
+        "mgv_sink_read": (st, [c_void_p, c_uint32, c_void_p, c_uint64, POINTER(c_uint64)]),
+        "mgv_gen_uniform": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_int64, c_uint64, c_void_p]),
+        "mgv_gen_perm": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
+        "mgv_gen_probe_keys": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint64, c_uint64, c_uint32,
+                                    c_int64, c_uint64, POINTER(c_uint64), c_void_p]),
+        "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str) -> None:
+    if status != OK:
+        detail = load().mgv_last_error_string().decode(errors="replace")
+        raise MgvError(status, where, detail)
+
+
+def _call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args), name)
+
+
+def _stream(stream) -> c_void_p:
+    if stream is None:
+        return c_void_p(0)
+    if isinstance(stream, int):
+        return c_void_p(stream)
+    return c_void_p(stream.cuda_stream)  # torch.cuda.Stream
+
+
+def _ptr(x) -> int:
+    """Device address of a torch tensor or a raw integer pointer."""
+    return x if isinstance(x, int) else x.data_ptr()
+
+
+class Context:
+    """mgv_ctx: one device, one stream, one device error word."""
+
+    def __init__(self, device: int = 0):
+        h = c_void_p()
+        _call("mgv_ctx_create", device, byref(h))
+        self.h = h
+        self.device = device
+
+    def info(self) -> CtxInfo:
+        i = CtxInfo()
+        _call("mgv_ctx_info_get", self.h, byref(i))
+        return i
+
+    def sync(self, stream=None) -> None:
+        _call("mgv_ctx_sync", self.h, _stream(stream))
+
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        _call("mgv_ctx_get_tuning", self.h, byref(t))
+        return t
+
+    def set_tuning(self, **kw) -> Tuning:
+        t = self.tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _call("mgv_ctx_set_tuning", self.h, byref(t))
+        return t
+
+    @property
+    def launches(self) -> int:
+        return int(load().mgv_ctx_launches(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            load().mgv_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # seeded columns ---------------------------------------------------
+    def gen_uniform(self, dst, n, seed, stream_id, lo, rng, stream=None):
+        _call("mgv_gen_uniform", self.h, c_void_p(_ptr(dst)), n, seed, stream_id, lo, rng, _stream(stream))
+
+    def gen_perm(self, dst, n, seed, stream=None):
+        _call("mgv_gen_perm", self.h, c_void_p(_ptr(dst)), n, seed, _stream(stream))
+
+    def gen_probe_keys(self, dst, n, seed, build_seed, nbuild, hit_num, miss_lo, miss_range, stream=None) -> int:
+        hits = c_uint64()
+        _call("mgv_gen_probe_keys", self.h, c_void_p(_ptr(dst)), n, seed, build_seed, nbuild, hit_num,
+              miss_lo, miss_range, byref(hits), _stream(stream))
+        return hits.value
+
+    def gen_zipf(self, dst, n, seed, stream_id, groups, s=1.0, stream=None):
+        _call("mgv_gen_zipf", self.h, c_void_p(_ptr(dst)), n, seed, stream_id, groups, s, _stream(stream))
+
+
+class Pool:
+    """mgv_pool: the device buffer pool (buffer_pool / buffer_manager)."""
+
+    def __init__(self, ctx: Context, nbuffers: int, capacity: int, ncols: int):
+        h = c_void_p()
+        _call("mgv_pool_create", ctx.h, nbuffers, capacity, ncols, byref(h))
+        self.h, self.ctx = h, ctx
+
+    def acquire(self, timeout_us: int = 100000):
+        b = POINTER(Buffer)()
+        _call("mgv_buffer_acquire", self.h, timeout_us, byref(b))
+        return b
+
+    def try_acquire(self, timeout_us: int = 0):
+        b = POINTER(Buffer)()
+        st = load().mgv_buffer_acquire(self.h, timeout_us, byref(b))
+        return st, (b if st == OK else None)
+
+    def release(self, b) -> None:
+        _call("mgv_buffer_release", self.h, b)
+
+    def register_producer(self) -> None:
+        _call("mgv_pool_register_producer", self.h)
+
+    def unregister_producer(self) -> None:
+        _call("mgv_pool_unregister_producer", self.h)
+
+    def stats(self) -> PoolStats:
+        s = PoolStats()
+        _call("mgv_pool_stats_get", self.h, byref(s))
+        return s
+
+    def destroy(self) -> None:
+        if self.h:
+            load().mgv_pool_destroy(self.h)
+            self.h = None
+
+
+def buffer_write(b, col: int, src_ptr: int, rows: int, stream=None) -> None:
+    _call("mgv_buffer_write", b, col, c_void_p(src_ptr), rows, _stream(stream))
+
+
+def buffer_read(b, col: int, dst_ptr: int, rows: int, stream=None) -> None:
+    _call("mgv_buffer_read", b, col, c_void_p(dst_ptr), rows, _stream(stream))
+
+
+class Op:
+    """mgv_op: one operator of a push chain (d_operator_t)."""
+
+    def __init__(self, ctx: Context, h: c_void_p, kind: str, parent: "Op | None" = None):
+        self.ctx, self.h, self.kind, self.parent = ctx, h, kind, parent
+
+    # construction --------------------------------------------------------
+    @classmethod
+    def select(cls, ctx, col: int, bound: int, parent: "Op") -> "Op":
+        h = c_void_p()
+        _call("mgv_op_create_select", ctx.h, byref(SelectDesc(col, bound)), parent.h, byref(h))
+        return cls(ctx, h, "select", parent)
+
+    @classmethod
+    def aggregate(cls, ctx, sum_col_a: int = -1, sum_col_b: int = -1) -> "Op":
+        h = c_void_p()
+        _call("mgv_op_create_aggregate", ctx.h, byref(AggregateDesc(sum_col_a, sum_col_b)), byref(h))
+        return cls(ctx, h, "aggregate")
+
+    @classmethod
+    def hash_build(cls, ctx, key_col: int, payload_col: int, expected_rows: int, load_factor: float = 0.0) -> "Op":
+        h = c_void_p()
+        d = HashBuildDesc(key_col, payload_col, expected_rows, load_factor, 0)
+        _call("mgv_op_create_hash_build", ctx.h, byref(d), byref(h))
+        return cls(ctx, h, "hash_build")
+
+    @classmethod
+    def hash_probe(cls, ctx, key_col: int, build: "Op", parent: "Op") -> "Op":
+        h = c_void_p()
+        _call("mgv_op_create_hash_probe", ctx.h, byref(HashProbeDesc(key_col, 0, build.h.value)), parent.h, byref(h))
+        op = cls(ctx, h, "hash_probe", parent)
+        op.build = build
+        return op
+
+    @classmethod
+    def sink(cls, ctx, pool: Pool, max_buffers: int = 0) -> "Op":
+        h = c_void_p()
+        _call("mgv_op_create_sink", ctx.h, byref(SinkDesc(pool.h.value, max_buffers, 0)), byref(h))
+        op = cls(ctx, h, "sink")
+        op.pool = pool
+        return op
+
+    # lifecycle -------------------------------------------------------------
+    def open(self, stream=None) -> None:
+        _call("mgv_op_open", self.h, _stream(stream))
+
+    def consume(self, buf, stream=None) -> None:
+        _call("mgv_op_consume", self.h, buf, _stream(stream))
+
+    def consume_columns(self, cols, rows: int, stream=None) -> None:
+        arr = (c_void_p * max(1, len(cols)))(*[_ptr(c) for c in cols])
+        _call("mgv_op_consume_columns", self.h, arr, len(cols), rows, _stream(stream))
+
+    def close(self, stream=None) -> None:
+        _call("mgv_op_close", self.h, _stream(stream))
+
+    def try_close(self, stream=None) -> int:
+        return load().mgv_op_close(self.h, _stream(stream))
+
+    def result(self):
+        if self.kind == "aggregate":
+            r = AggResult()
+            _call("mgv_op_result", self.h, byref(r), ctypes.sizeof(r), None)
+            return r.count, r.sum
+        if self.kind == "hash_build":
+            r = HashBuildInfo()
+            _call("mgv_op_result", self.h, byref(r), ctypes.sizeof(r), None)
+            return r
+        if self.kind == "sink":
+            r = c_uint64()
+            _call("mgv_op_result", self.h, byref(r), ctypes.sizeof(r), None)
+            return r.value
+        raise MgvError(EINVAL, "result", f"{self.kind} has no result")
+
+    def sink_read(self, col: int, dst_ptr: int, max_rows: int) -> int:
+        n = c_uint64()
+        _call("mgv_sink_read", self.h, col, c_void_p(dst_ptr), max_rows, byref(n))
+        return n.value
+
+    def destroy(self) -> None:
+        if self.h:
+            load().mgv_op_destroy(self.h)
+            self.h = None
+
+
+# ---- reference-style plans (src/main9.cu:202-367) ---------------------------
+
+def create_sum_select_pipeline(ctx: Context, bound: int, filter_col: int = 0, sum_col: int = 0):
+    """select(cols[filter_col] <= bound) -> aggregate(COUNT, SUM(cols[sum_col])).
+
+    create_sum_select_pipeline (src/main9.cu:202-226) with the aggregate
+    widened to COUNT + int64 SUM.  Returns (head, aggregate)."""
+    agg = Op.aggregate(ctx, sum_col, -1)
+    sel = Op.select(ctx, filter_col, bound, agg)
+    return sel, agg
+
+
+def create_count_join_1G_pipeline(ctx: Context, build_rows: int, load_factor: float = 0.0,
+                                  build_filter_bound: int | None = None):
+    """Hash join on one GPU (create_count_join_1G_pipeline, src/main9.cu:326-367).
+
+    Build side columns: (key, payload); probe side columns: (key, payload).
+    Returns (build_head, build, probe_head, aggregate) where the aggregate
+    yields COUNT(matches) and SUM(build payload + probe payload).  With
+    build_filter_bound the build side is select(key <= bound) -> build,
+    as the reference's CPU join filters its build rows (src/main8.cu:87)."""
+    hb = Op.hash_build(ctx, 0, 1, build_rows, load_factor)
+    bhead = Op.select(ctx, 0, build_filter_bound, hb) if build_filter_bound is not None else hb
+    agg = Op.aggregate(ctx, 1, 2)  # probe payload (col 1) + build payload (appended col 2)
+    probe = Op.hash_probe(ctx, 0, hb, agg)
+    return bhead, hb, probe, agg

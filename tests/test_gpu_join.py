@@ -1,0 +1,279 @@
+"""Hash build + probe on the GPU against the oracle's chained-table join.
+
+The oracle restates sum_hashjoin_select_cpu (src/main8.cu:84-103), itself
+pinned to the reference's compiled CPU code by tests/test_oracle_golden.py.
+Cases follow the reference's join checks (src/main8.cu:322-355: match count
+against the CPU join) plus the configurations' known answers.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import mgv
+import pyoracle as po
+from gpu_util import dev, i32
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.json")))
+HIT = 3865470566  # 0.9 * 2^32
+
+
+def join_count_sum(ctx, torch, bk, bp, pk, pp, load_factor=0.0, build_filter=None, expected=None):
+    """Run build + probe -> aggregate(COUNT, SUM(bp + pp)); returns (count, sum, info)."""
+    n, m = bk.size, pk.size
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, expected or max(n, 1), load_factor, build_filter)
+    bhead.open()
+    if n:
+        bhead.consume_columns([dev(torch, bk), dev(torch, bp)], n)
+    bhead.close()
+    info = hb.result()
+    probe.open()
+    if m:
+        probe.consume_columns([dev(torch, pk), dev(torch, pp)], m)
+    probe.close()
+    r = agg.result()
+    for o in (probe, agg, bhead, hb):
+        o.destroy()
+    return r[0], r[1], info
+
+
+def config2_inputs(nb, npb, seed=0x5EED0002):
+    bk = po.gen_perm(nb, seed)
+    bp = po.gen_uniform(nb, seed, 1, 0, 1 << 20)
+    pk, hits = po.gen_probe_keys(npb, 0x5EED0003, seed, nb, HIT, nb, (1 << 31) - nb)
+    pp = po.gen_uniform(npb, 0x5EED0003, 2, 0, 1 << 20)
+    return bk, bp, pk, pp, hits
+
+
+PROBE_VARIANTS = [dict(probe_kernel=0), dict(probe_kernel=1), dict(probe_kernel=2, probe_rows_per_thread=8, probe_stages=2),
+                  dict(probe_kernel=2, probe_rows_per_thread=4, probe_stages=6),
+                  dict(probe_kernel=2, probe_rows_per_thread=4, probe_stages=4, probe_ctas_per_sm=3),
+                  dict(probe_kernel=2, probe_rows_per_thread=8, probe_stages=4, probe_ctas_per_sm=1)]
+
+
+@pytest.fixture
+def tuned(ctx, request):
+    """Apply a probe tuning for one test and restore the default after it."""
+    old = ctx.tuning()
+    keep = {k: getattr(old, k) for k in ("probe_kernel", "probe_rows_per_thread", "probe_stages", "probe_ctas_per_sm")}
+    ctx.set_tuning(**request.param)
+    yield request.param
+    ctx.set_tuning(**keep)
+
+
+@pytest.mark.parametrize("tuned", PROBE_VARIANTS, indirect=True, ids=lambda v: "_".join(f"{k[6:]}{x}" for k, x in v.items()))
+@pytest.mark.parametrize("nb,npb", [(1 << 10, 1 << 12), (1 << 16, 1 << 20), (1000003, 3000017), (77, 1000)])
+def test_config2_shape(ctx, torch_cuda, tuned, nb, npb):
+    bk, bp, pk, pp, hits = config2_inputs(nb, npb)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
+    want = po.Chain(bk, bp).probe_agg(pk, pp)
+    assert (cnt, s) == want
+    assert cnt == hits  # known answer: every hit row matches exactly one unique key
+    assert info.rows == nb and info.has_duplicates == 0
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3])
+def test_unaligned_probe_columns(ctx, torch_cuda, offset):
+    """Columns that are not 16-byte aligned take the register-prefetch kernel."""
+    torch = torch_cuda
+    bk, bp, pk, pp, hits = config2_inputs(1 << 12, 50001)
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, bk.size)
+    bhead.open(); bhead.consume_columns([dev(torch, bk), dev(torch, bp)], bk.size); bhead.close()
+    dpk = dev(torch, np.concatenate([np.zeros(offset, np.int32), pk]))
+    dpp = dev(torch, np.concatenate([np.zeros(offset, np.int32), pp]))
+    probe.open()
+    probe.consume_columns([dpk.data_ptr() + 4 * offset, dpp.data_ptr() + 4 * offset], pk.size)
+    probe.close()
+    assert agg.result() == po.Chain(bk, bp).probe_agg(pk, pp)
+    for o in (probe, agg, hb):
+        o.destroy()
+
+
+@pytest.mark.parametrize("tuned", PROBE_VARIANTS[1:4], indirect=True, ids=lambda v: "_".join(f"{k[6:]}{x}" for k, x in v.items()))
+@pytest.mark.parametrize("mode", [(-1, -1), (2, -1), (1, -1), (1, 2)])
+def test_sum_modes(ctx, torch_cuda, tuned, mode):
+    """COUNT with SUM of nothing, build payload, probe payload, or both."""
+    torch = torch_cuda
+    bk = po.gen_uniform(5000, 0x5EED0604, 0, 0, 4000)
+    bp = po.gen_uniform(5000, 0x5EED0604, 1, -(1 << 31), 1 << 32)
+    pk = po.gen_uniform(70001, 0x5EED0604, 2, 0, 4500)
+    pp = po.gen_uniform(70001, 0x5EED0604, 3, -(1 << 31), 1 << 32)
+    hb = mgv.Op.hash_build(ctx, 0, 1, bk.size)
+    hb.open(); hb.consume_columns([dev(torch, bk), dev(torch, bp)], bk.size); hb.close()
+    agg = mgv.Op.aggregate(ctx, *mode)
+    pr = mgv.Op.hash_probe(ctx, 0, hb, agg)
+    pr.open(); pr.consume_columns([dev(torch, pk), dev(torch, pp)], pk.size); pr.close()
+    add_b = 2 in mode
+    add_p = 1 in mode
+    assert agg.result() == po.Chain(bk, bp).probe_agg(pk, pp, add_b, add_p)
+    for o in (pr, agg, hb):
+        o.destroy()
+
+
+def test_config2_full_size(ctx, torch_cuda):
+    """Build 2^22 unique keys, probe 2^26 (the headline configuration)."""
+    torch = torch_cuda
+    nb, npb = 1 << 22, 1 << 26
+    bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+    bp = torch.empty(nb, dtype=torch.int32, device="cuda")
+    pk = torch.empty(npb, dtype=torch.int32, device="cuda")
+    pp = torch.empty(npb, dtype=torch.int32, device="cuda")
+    ctx.gen_perm(bk, nb, 0x5EED0002)
+    ctx.gen_uniform(bp, nb, 0x5EED0002, 1, 0, 1 << 20)
+    hits = ctx.gen_probe_keys(pk, npb, 0x5EED0003, 0x5EED0002, nb, HIT, nb, (1 << 31) - nb)
+    ctx.gen_uniform(pp, npb, 0x5EED0003, 2, 0, 1 << 20)
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb)
+    bhead.open(); bhead.consume_columns([bk, bp], nb); bhead.close()
+    probe.open(); probe.consume_columns([pk, pp], npb); probe.close()
+    cnt, s = agg.result()
+    hbk, hbp = bk.cpu().numpy(), bp.cpu().numpy()
+    hpk, hpp = pk.cpu().numpy(), pp.cpu().numpy()
+    want = po.Chain(hbk, hbp).probe_agg_mt(hpk, hpp, os.cpu_count() or 1)
+    assert cnt == hits
+    assert (cnt, s) == want
+    # sorted match multiset on the first 2^16 probe rows
+    pool = mgv.Pool(ctx, 8, 1 << 16, 3)
+    sink = mgv.Op.sink(ctx, pool)
+    pe = mgv.Op.hash_probe(ctx, 0, hb, sink)
+    pe.open(); pe.consume_columns([pk, pp], 1 << 16); pe.close()
+    rows = sink.result()
+    out = [torch.empty(rows, dtype=torch.int32, device="cuda") for _ in range(3)]
+    for c in range(3):
+        sink.sink_read(c, out[c].data_ptr(), rows)
+    got = np.stack([out[0].cpu().numpy(), out[2].cpu().numpy(), out[1].cpu().numpy()], 1)  # key, bp, pp
+    got = got[np.lexsort((got[:, 2], got[:, 1], got[:, 0]))]
+    want_ms = po.Chain(hbk, hbp).probe_emit(hpk[:1 << 16], hpp[:1 << 16])
+    assert np.array_equal(got, want_ms)
+    for o in (pe, sink, probe, agg, bhead, hb):
+        o.destroy()
+    pool.destroy()
+
+
+@pytest.mark.parametrize("lf", [0.25, 0.5, 0.75, 0.95])
+def test_duplicates_and_load_factors(ctx, torch_cuda, lf):
+    """Duplicate build keys: every duplicate matches (hashjoin.cu:148-162)."""
+    nb, npb = 20000, 50000
+    bk = po.gen_uniform(nb, 0x5EED0601, 0, 0, 3000)
+    bp = po.gen_uniform(nb, 0x5EED0601, 1, -(1 << 31), 1 << 32)
+    pk = po.gen_uniform(npb, 0x5EED0601, 2, -100, 3200)
+    pp = po.gen_uniform(npb, 0x5EED0601, 3, -(1 << 31), 1 << 32)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp, load_factor=lf)
+    assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+    assert info.has_duplicates == 1
+
+
+def test_reserved_key_int32_min(ctx, torch_cuda):
+    """INT32_MIN is the table's empty marker; such rows still join exactly."""
+    mn = -(1 << 31)
+    bk = np.array([mn, 5, mn, 7, 5, mn, 2147483647], np.int32)
+    bp = np.array([1, 2, 3, 4, 5, 6, 7], np.int32)
+    pk = np.array([mn, 5, 7, 8, mn, 2147483647, 0], np.int32)
+    pp = np.array([10, 20, 30, 40, 50, 60, 70], np.int32)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
+    assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+    assert info.reserved_key_rows == 3
+
+
+@pytest.mark.parametrize("nb,npb", [(0, 100), (100, 0), (1, 1), (129, 4097)])
+def test_empty_and_tiny(ctx, torch_cuda, nb, npb):
+    bk = po.gen_uniform(nb, 0x5EED0602, 0, 0, 50)
+    bp = po.gen_uniform(nb, 0x5EED0602, 1, 0, 1 << 20)
+    pk = po.gen_uniform(npb, 0x5EED0602, 2, 0, 60)
+    pp = po.gen_uniform(npb, 0x5EED0602, 3, 0, 1 << 20)
+    cnt, s, _ = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
+    assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN["cases"] if c["op"] == "hashjoin"],
+                         ids=lambda c: f"b{c['build']['n']}_p{c['probe']['n']}")
+def test_golden_count_join_select(ctx, torch_cuda, case):
+    """select(key <= 5000) -> build; probe -> COUNT == sum_hashjoin_select_cpu."""
+    b, p = case["build"], case["probe"]
+    a = po.gen_uniform(b["n"], b["seed"], b["stream"], b["lo"], b["range"])
+    q = po.gen_uniform(p["n"], p["seed"], p["stream"], p["lo"], p["range"])
+    zeros_a, zeros_q = np.zeros(a.size, np.int32), np.zeros(q.size, np.int32)
+    cnt, _, _ = join_count_sum(ctx, torch_cuda, a, zeros_a, q, zeros_q, build_filter=case["build_filter"],
+                               expected=max(a.size, 1))
+    assert i32(cnt) == case["count_int32"]
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN["cases"] if c["op"] == "selfjoin"], ids=lambda c: f"n{c['input']['n']}")
+def test_golden_selfjoin(ctx, torch_cuda, case):
+    """select(a <= 5000) joined with itself == sum_selfjoin_select_cpu (sum of hist^2)."""
+    s = case["input"]
+    a = po.gen_uniform(s["n"], s["seed"], s["stream"], s["lo"], s["range"])
+    z = np.zeros(a.size, np.int32)
+    # build: select(a <= 5000) -> hash_build; probe: select(a <= 5000) -> hash_probe -> sink is
+    # not needed: probe every row and let the build side's filter decide, then subtract nothing:
+    # rows a > 5000 never match a build key <= 5000.
+    cnt, _, _ = join_count_sum(ctx, torch_cuda, a, z, a, z, build_filter=5000, expected=max(a.size, 1))
+    assert i32(cnt) == case["count_int32"]
+
+
+def test_table_full_is_reported(ctx, torch_cuda):
+    bk = np.arange(1000, dtype=np.int32)
+    bp = np.zeros(1000, np.int32)
+    hb = mgv.Op.hash_build(ctx, 0, 1, 10, 0.5)
+    hb.open()
+    hb.consume_columns([dev(torch_cuda, bk), dev(torch_cuda, bp)], 1000)
+    with pytest.raises(mgv.MgvError) as e:
+        hb.close()
+    assert e.value.status == mgv.ENOMEM
+    hb.destroy()
+
+
+def test_probe_before_build_closed_is_rejected(ctx):
+    hb = mgv.Op.hash_build(ctx, 0, 1, 100)
+    agg = mgv.Op.aggregate(ctx, 1, 2)
+    pr = mgv.Op.hash_probe(ctx, 0, hb, agg)
+    with pytest.raises(mgv.MgvError) as e:
+        pr.open()
+    assert e.value.status == mgv.ESTATE
+    for o in (pr, agg, hb):
+        o.destroy()
+
+
+def test_duplicate_emit_multiset(ctx, torch_cuda):
+    torch = torch_cuda
+    nb, npb = 3000, 5000
+    bk = po.gen_uniform(nb, 0x5EED0603, 0, 0, 500)
+    bp = po.gen_uniform(nb, 0x5EED0603, 1, 0, 1 << 20)
+    pk = po.gen_uniform(npb, 0x5EED0603, 2, 0, 600)
+    pp = po.gen_uniform(npb, 0x5EED0603, 3, 0, 1 << 20)
+    hb = mgv.Op.hash_build(ctx, 0, 1, nb)
+    hb.open(); hb.consume_columns([dev(torch, bk), dev(torch, bp)], nb); hb.close()
+    pool = mgv.Pool(ctx, 64, 1 << 14, 3)
+    sink = mgv.Op.sink(ctx, pool)
+    pe = mgv.Op.hash_probe(ctx, 0, hb, sink)
+    pe.open(); pe.consume_columns([dev(torch, pk), dev(torch, pp)], npb); pe.close()
+    rows = sink.result()
+    out = [torch.empty(max(rows, 1), dtype=torch.int32, device="cuda") for _ in range(3)]
+    for c in range(3):
+        sink.sink_read(c, out[c].data_ptr(), rows)
+    got = np.stack([out[0].cpu().numpy()[:rows], out[2].cpu().numpy()[:rows], out[1].cpu().numpy()[:rows]], 1)
+    got = got[np.lexsort((got[:, 2], got[:, 1], got[:, 0]))]
+    assert np.array_equal(got, po.Chain(bk, bp).probe_emit(pk, pp))
+    for o in (pe, sink, hb):
+        o.destroy()
+    pool.destroy()
+
+
+@pytest.mark.parametrize("tuned", PROBE_VARIANTS[2:], indirect=True, ids=lambda v: "_".join(f"{k[6:]}{x}" for k, x in v.items()))
+def test_staged_probe_is_repeatable(ctx, torch_cuda, tuned):
+    """Many probe passes over one table: every pass exact (catches races in
+    the shared-memory stage ring and the continuation queue)."""
+    torch = torch_cuda
+    nb, npb = 1 << 20, 1 << 22
+    bk, bp, pk, pp, hits = config2_inputs(nb, npb)
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb)
+    bhead.open(); bhead.consume_columns([dev(torch, bk), dev(torch, bp)], nb); bhead.close()
+    d = [dev(torch, pk), dev(torch, pp)]
+    want = po.Chain(bk, bp).probe_agg(pk, pp)
+    for _ in range(8):
+        probe.open(); probe.consume_columns(d, npb); probe.close()
+        assert agg.result() == want
+    for o in (probe, agg, hb):
+        o.destroy()
