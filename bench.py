@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--rows-per-thread", type=int, default=None)
     ap.add_argument("--stages", type=int, default=None)
     ap.add_argument("--ctas-per-sm", type=int, default=None)
+    ap.add_argument("--gather-ceiling", action="store_true",
+                    help="measure the random 32-byte bucket-read ceiling instead of the join")
     ap.add_argument("--settle-s", type=float, default=1.0, help="untimed steps before timing, in seconds")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -204,6 +206,18 @@ def main():
 
     import torch
     import mgv
+
+    if args.gather_ceiling:
+        ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
+        out = []
+        for tb in (1 << 20, 32 << 20, 64 << 20):
+            for c in (2, 4):
+                ms = ctx.diag_random_gather(tb, args.probe_rows, c, 20)
+                out.append({"table_bytes": tb, "ctas_per_sm": c, "ms_per_pass": ms,
+                            "gather_per_s": args.probe_rows / (ms / 1e3)})
+        print(json.dumps({"gather_ceiling": out, "rows": args.probe_rows}), flush=True)
+        ctx.close()
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

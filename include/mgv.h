@@ -272,6 +272,16 @@ mgv_status mgv_gen_probe_keys(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t s
 mgv_status mgv_gen_zipf(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint32_t stream_id,
                         uint32_t groups, double s, void *stream);
 
+/* ---- diagnostics ------------------------------------------------------ */
+
+/* Random 32-byte bucket-read ceiling: times `reps` passes of n hashed
+ * 32-byte loads into a table of table_bytes (R = 4 loads in flight per
+ * thread, ctas_per_sm CTAs of 256 threads per SM) and returns the mean
+ * milliseconds per pass.  The bound every hash probe is measured against;
+ * no reference counterpart. */
+mgv_status mgv_diag_random_gather(mgv_ctx *ctx, uint64_t table_bytes, uint64_t n, uint32_t ctas_per_sm,
+                                  uint32_t reps, double *ms_per_pass);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,18 +45,30 @@ static cudaStream_t pick_stream(Context* ctx, void* stream) {
     return stream ? (cudaStream_t)stream : ctx->stream;
 }
 
-// Reads and clears the context's device error word after `s` completes.
-static mgv_status check_device(Context* ctx, cudaStream_t s) {
-    MGV_CUDA_TRY(cudaStreamSynchronize(s));
-    uint32_t h[2] = {0, 0};
-    MGV_CUDA_TRY(cudaMemcpy(h, ctx->d_err, sizeof(h), cudaMemcpyDeviceToHost));
+// Maps a device error word to a status (and clears it on the device).
+static mgv_status report_device_error(Context* ctx, const uint32_t* h, cudaStream_t s) {
     if (h[0] == 0) return MGV_OK;
-    MGV_CUDA_TRY(cudaMemset(ctx->d_err, 0, sizeof(h)));
+    MGV_CUDA_TRY(cudaMemsetAsync(ctx->d_err, 0, 2 * sizeof(uint32_t), s));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
     char msg[128];
     std::snprintf(msg, sizeof(msg), "device error word %u (site %u)", h[0], h[1]);
     if (h[0] == MGV_ENOMEM) return fail(MGV_ENOMEM, std::string(msg) + ": table, pool or output full");
     if (h[0] == MGV_ETIMEDOUT) return fail(MGV_ETIMEDOUT, std::string(msg) + ": bounded wait ran out");
     return fail(MGV_EDEVICE, msg);
+}
+
+// Waits for `s`, then reports and clears the context's device error word.
+static mgv_status check_device(Context* ctx, cudaStream_t s) {
+    uint32_t w[2];
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);  // h_stage is shared by the context
+        uint32_t* h = reinterpret_cast<uint32_t*>(ctx->h_stage);
+        MGV_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        MGV_CUDA_TRY(cudaStreamSynchronize(s));
+        w[0] = h[0];
+        w[1] = h[1];
+    }
+    return report_device_error(ctx, w, s);
 }
 
 extern "C" {
@@ -96,7 +108,9 @@ mgv_status mgv_ctx_create(int device, mgv_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreate(&c->stream);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_stage, 8 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
+        if (c->h_stage) cudaFreeHost(c->h_stage);
         if (c->d_err) cudaFree(c->d_err);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -111,6 +125,7 @@ mgv_status mgv_ctx_destroy(mgv_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_err);
+    cudaFreeHost(ctx->h_stage);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MGV_OK;
@@ -368,6 +383,12 @@ mgv_status mgv_op_create_aggregate(mgv_ctx* ctx, const mgv_aggregate_desc* d, mg
     o->agg = *d;
     mgv_status st = dev_alloc(o, (void**)&o->d_acc, 2 * sizeof(unsigned long long));
     if (st != MGV_OK) { delete o; return st; }
+    cudaError_t e = cudaMallocHost(&o->h_res, 4 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        for (void* p : o->allocs) cudaFree(p);
+        delete o;
+        return cuda_fail(e, "mgv_op_create_aggregate");
+    }
     *out = o;
     return MGV_OK;
 }
@@ -457,6 +478,7 @@ mgv_status mgv_op_destroy(mgv_op* o) {
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
     if (o->kind == OpKind::Sink) sink_return_buffers(o);
+    if (o->h_res) cudaFreeHost(o->h_res);
     for (void* p : o->allocs) cudaFree(p);
     delete o;
     return MGV_OK;
@@ -556,6 +578,17 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
     o->state = OpState::Closed;
     mgv_status st = MGV_OK;
     if (!o->parent) {  // terminal: wait, check the device error word, read results
+        if (o->kind == OpKind::Aggregate) {
+            // one pinned landing zone, one synchronisation
+            unsigned long long* h = o->h_res;
+            MGV_CUDA_TRY(cudaMemcpyAsync(h, o->ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(h + 2, o->d_acc, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
+            o->agg_result.count = (int64_t)h[2];
+            o->agg_result.sum = (int64_t)h[3];
+            return report_device_error(o->ctx, w, s);
+        }
         st = check_device(o->ctx, s);
         mgv_status st2 = op_finish(o, s);
         if (st == MGV_OK) st = st2;

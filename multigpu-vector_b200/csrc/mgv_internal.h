@@ -90,8 +90,10 @@ struct Context {
     cudaDeviceProp prop{};
     cudaStream_t stream = nullptr;
     uint32_t* d_err = nullptr;      // device error word [code, detail]
+    // pinned landing zone for close(): [0..1] error word, [2..] result words
+    unsigned long long* h_stage = nullptr;
     std::atomic<uint64_t> launches{0};
-    mgv_tuning tuning{0u, 4u, 4u, 0u, 0.5f, {0u, 0u, 0u}};
+    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, {0u, 0u, 0u}};
     std::mutex mu;
 };
 
@@ -108,6 +110,7 @@ struct Op {
     // aggregate
     mgv_aggregate_desc agg{};
     unsigned long long* d_acc = nullptr;    // [count, sum]
+    unsigned long long* h_res = nullptr;    // pinned: [error word, count, sum]
     mgv_agg_result agg_result{};
     // hash build
     mgv_hash_build_desc hb{};

@@ -34,22 +34,26 @@ namespace {
 
 constexpr int kConsumerWarps = 8;
 constexpr int kThreads = (kConsumerWarps + 1) * 32;
-// continuation queue entries per consumer warp: room for two full rounds
-template <int R>
-constexpr int queue_len() { return 32 * (R + 1) <= 128 ? 256 : 512; }
 constexpr uint32_t kWaitTries = 1u << 24;
 
+// continuation queue entries per consumer warp: room for two full rounds
+template <int R>
+constexpr int queue_len() { return 32 * (R + 1) <= 160 ? 256 : 512; }
+
 struct Acc {
-    unsigned long long cnt, sum;
+    uint32_t cnt;            // matches of this thread (fits: rows per thread < 2^32)
+    unsigned long long sum;  // two's-complement int64
 };
 
-// Per-warp continuation queue (ring) in shared memory.
+// Per-warp continuation queue (ring) in shared memory.  `tail` is a shared
+// counter bumped with atomicAdd by the (few) lanes that append; `head` is
+// warp-uniform and private to the warp.
 struct ContQueue {
     int32_t* key;
     int32_t* pay;
     uint32_t* bucket;
-    uint32_t head;   // warp-uniform
-    uint32_t count;  // warp-uniform
+    uint32_t* tail;
+    uint32_t head;
 };
 
 __device__ __forceinline__ uint32_t next_bucket(uint32_t b, uint32_t nb) { return (b + 1 == nb) ? 0u : b + 1; }
@@ -57,47 +61,66 @@ __device__ __forceinline__ uint32_t next_bucket(uint32_t b, uint32_t nb) { retur
 // Fold one bucket's matches for (key, pay); returns whether the run goes on.
 template <bool UNIQUE, bool ADD_BP, bool ADD_PP>
 __device__ __forceinline__ bool fold(const uint32_t (&w)[8], int32_t key, int32_t pay, Acc& a) {
-    uint32_t mc;
-    long long ms;
-    bool more;
-    match_bucket<UNIQUE>(w, key, mc, ms, more);
-    a.cnt += mc;
-    long long add = 0;
-    if (ADD_BP) add += ms;
-    if (ADD_PP) add += (long long)mc * pay;
-    a.sum += (unsigned long long)add;
-    return more;
-}
-
-// Warp-wide append of the lanes with `push` set.  Callers keep the queue
-// below Q - 32 * (R + 1) before a round, so an append always fits.
-template <int Q>
-__device__ __forceinline__ void enqueue(ContQueue& q, bool push, int32_t key, int32_t pay, uint32_t b) {
-    const unsigned m = __ballot_sync(0xffffffffu, push);
-    if (m == 0) return;
-    const uint32_t lane = lane_id();
-    if (push) {
-        const uint32_t idx = (q.head + q.count + __popc(m & ((1u << lane) - 1u))) & (Q - 1);
-        q.key[idx] = key;
-        q.pay[idx] = pay;
-        q.bucket[idx] = b;
+    const uint32_t k = (uint32_t)key;
+    const bool m0 = w[0] == k, m1 = w[2] == k, m2 = w[4] == k, m3 = w[6] == k;
+    const bool full = w[6] != (uint32_t)kEmptyKey;
+    if (UNIQUE) {
+        const bool f = m0 | m1 | m2 | m3;
+        long long v = 0;
+        if (ADD_BP) v += (int32_t)(m0 ? w[1] : m1 ? w[3] : m2 ? w[5] : w[7]);
+        if (ADD_PP) v += pay;
+        a.cnt += f;
+        if (ADD_BP || ADD_PP) a.sum += f ? (unsigned long long)v : 0ull;
+        return !f && full;
     }
-    q.count += __popc(m);
-    __syncwarp();
+    const uint32_t mc = (uint32_t)m0 + m1 + m2 + m3;
+    a.cnt += mc;
+    long long v = 0;
+    if (ADD_BP)
+        v += (m0 ? (long long)(int32_t)w[1] : 0ll) + (m1 ? (long long)(int32_t)w[3] : 0ll) +
+             (m2 ? (long long)(int32_t)w[5] : 0ll) + (m3 ? (long long)(int32_t)w[7] : 0ll);
+    if (ADD_PP) v += (long long)mc * pay;
+    if (ADD_BP || ADD_PP) a.sum += (unsigned long long)v;
+    return full;
 }
 
-// One round for a warp: R rows per lane (valid bits in `valid`) plus, when
-// the queue holds a batch (or `drain`), one continuation per lane.
+template <int Q>
+__device__ __forceinline__ void enqueue(const ContQueue& q, int32_t key, int32_t pay, uint32_t b) {
+    const uint32_t pos = atomicAdd(q.tail, 1u) & (Q - 1);
+    q.key[pos] = key;
+    q.pay[pos] = pay;
+    q.bucket[pos] = b;
+}
+
+// Probe rows of the reserved key INT32_MIN against the side list.
+template <bool ADD_BP, bool ADD_PP>
+__device__ __forceinline__ void fold_reserved(const TableView& t, int32_t pay, Acc& a) {
+    const unsigned long long c = t.meta[0];
+    a.cnt += (uint32_t)c;
+    long long add = 0;
+    if (ADD_BP) add += (long long)t.meta[1];
+    if (ADD_PP) add += (long long)c * pay;
+    a.sum += (unsigned long long)add;
+}
+
+// One round for a warp: R rows per lane, row r of lane l at rk[32 r + l] /
+// rp[32 r + l] (so each read of the warp is one conflict-free 128-byte
+// wavefront; shared or global memory, valid bits in `valid`) plus, when the queue holds a batch
+// (or `drain`), one continuation per lane.  The rows are read twice --
+// to issue the bucket loads and again to fold the results -- so that no
+// key or payload stays in a register across the L2 latency.  Returns a
+// value that depends on every row read (for releasing a stage safely).
 template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
-__device__ __forceinline__ void round(const int32_t (&k)[R], const int32_t (&p)[R], uint32_t valid, ContQueue& q,
-                                      bool drain, const TableView& t, Acc& a) {
+__device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, uint32_t valid, ContQueue& q,
+                                          bool drain, const TableView& t, Acc& a) {
     const uint32_t lane = lane_id();
-    // take a continuation batch
+    __syncwarp();
+    const uint32_t avail = *((volatile uint32_t*)q.tail) - q.head;
     int32_t ck = 0, cp = 0;
     uint32_t cb = 0;
     bool has_c = false;
-    if (q.count >= 32 || (drain && q.count > 0)) {
-        const uint32_t m = q.count < 32 ? q.count : 32;
+    if (avail >= 32 || (drain && avail > 0)) {
+        const uint32_t m = avail < 32 ? avail : 32;
         if (lane < m) {
             const uint32_t idx = (q.head + lane) & (Q - 1);
             ck = q.key[idx];
@@ -105,52 +128,43 @@ __device__ __forceinline__ void round(const int32_t (&k)[R], const int32_t (&p)[
             cb = q.bucket[idx];
             has_c = true;
         }
-        q.head = (q.head + m) & (Q - 1);
-        q.count -= m;
-        __syncwarp();
+        q.head += m;
     }
     // issue every load of the round before looking at any of them
-    uint32_t hb[R];
     uint32_t w[R][8];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        hb[r] = bucket_of(k[r], t.nbuckets);
-        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * hb[r], w[r]);
-    }
+    for (int r = 0; r < R; ++r)
+        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * bucket_of(rk[32 * r], t.nbuckets), w[r]);
     uint32_t wc[8];
     if (has_c) ld_bucket(t.slots + 4ull * cb, wc);
+    __syncwarp();  // every lane has read its queue entry before anyone appends
 
+    uint32_t dep = 0;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        bool more = false;
-        if ((valid >> r) & 1u) {
-            if (k[r] == kEmptyKey) {
-                const unsigned long long c = t.meta[0];
-                a.cnt += c;
-                long long add = 0;
-                if (ADD_BP) add += (long long)t.meta[1];
-                if (ADD_PP) add += (long long)c * p[r];
-                a.sum += (unsigned long long)add;
-            } else {
-                more = fold<UNIQUE, ADD_BP, ADD_PP>(w[r], k[r], p[r], a);
-            }
+        if (!((valid >> r) & 1u)) continue;
+        const int32_t key = rk[32 * r];
+        const int32_t pay = ADD_PP ? rp[32 * r] : 0;
+        dep ^= (uint32_t)key ^ (uint32_t)pay;
+        if (key == kEmptyKey) {
+            fold_reserved<ADD_BP, ADD_PP>(t, pay, a);
+        } else if (fold<UNIQUE, ADD_BP, ADD_PP>(w[r], key, pay, a)) {
+            enqueue<Q>(q, key, pay, next_bucket(bucket_of(key, t.nbuckets), t.nbuckets));
         }
-        enqueue<Q>(q, more, k[r], p[r], next_bucket(hb[r], t.nbuckets));
     }
-    bool cmore = false;
-    if (has_c) cmore = fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a);
-    enqueue<Q>(q, cmore, ck, cp, next_bucket(cb, t.nbuckets));
+    if (has_c && fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a)) enqueue<Q>(q, ck, cp, next_bucket(cb, t.nbuckets));
+    return dep;
 }
 
 // Continuation-only rounds until a full round can no longer overflow the
 // queue.  They never grow it, and every run ends, so this terminates.
 template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
 __device__ __forceinline__ void make_room(ContQueue& q, const TableView& t, Acc& a, uint32_t limit) {
-    int32_t z[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) z[r] = 0;
-    for (uint32_t guard = 0; q.count > limit && guard < (1u << 24); ++guard)
-        round<R, Q, UNIQUE, ADD_BP, ADD_PP>(z, z, 0u, q, true, t, a);
+    for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
+        __syncwarp();
+        if (*((volatile uint32_t*)q.tail) - q.head <= limit) break;
+        round<R, Q, UNIQUE, ADD_BP, ADD_PP>(nullptr, nullptr, 0u, q, true, t, a);
+    }
 }
 
 template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
@@ -164,7 +178,8 @@ __global__ void __launch_bounds__(kThreads, MB)
     int32_t* sk = reinterpret_cast<int32_t*>(smem_raw);
     int32_t* sp = sk + S * T;
     int32_t* qbase = sp + (ADD_PP ? S * T : 0);
-    uint64_t* full = reinterpret_cast<uint64_t*>(qbase + 3 * kConsumerWarps * Q);
+    uint32_t* tails = reinterpret_cast<uint32_t*>(qbase + 3 * kConsumerWarps * Q);
+    uint64_t* full = reinterpret_cast<uint64_t*>(tails + kConsumerWarps);
     uint64_t* empty = full + S;
 
     const uint64_t nfull = n / T;
@@ -174,6 +189,7 @@ __global__ void __launch_bounds__(kThreads, MB)
     const uint32_t lane = lane_id();
     const uint32_t zero = (uint32_t)(n >> 63);  // 0 for every real row count
 
+    if (threadIdx.x < kConsumerWarps) tails[threadIdx.x] = 0;
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -184,7 +200,7 @@ __global__ void __launch_bounds__(kThreads, MB)
     }
     __syncthreads();
 
-    Acc a{0ull, 0ull};
+    Acc a{0u, 0ull};
     if (warp == kConsumerWarps) {
         // ---- producer warp: keep S tiles of the probe columns in flight ----
         if (lane == 0) {
@@ -211,68 +227,45 @@ __global__ void __launch_bounds__(kThreads, MB)
         q.key = qbase + warp * Q;
         q.pay = qbase + (kConsumerWarps + warp) * Q;
         q.bucket = reinterpret_cast<uint32_t*>(qbase + (2 * kConsumerWarps + warp) * Q);
+        q.tail = tails + warp;
         q.head = 0;
-        q.count = 0;
-        const int row0 = (warp * 32 + (int)lane) * R;
+        const int row0 = warp * 32 * R + (int)lane;
         bool ok = true;
         for (uint64_t i = 0; i < my_tiles; ++i) {
             const int s = (int)(i % S);
-            if (!mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1), kWaitTries)) {
-                ok = false;
-            }
+            if (!mbar_wait_bounded(&full[s], (uint32_t)((i / S) & 1), kWaitTries)) ok = false;
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) set_error(err, kDevTimeout, 12);
                 break;
             }
-            int32_t k[R], p[R];
-#pragma unroll
-            for (int r = 0; r < R; r += 4) {
-                const int4 v = *reinterpret_cast<const int4*>(sk + s * T + row0 + r);
-                k[r] = v.x; k[r + 1] = v.y; k[r + 2] = v.z; k[r + 3] = v.w;
-                if (ADD_PP) {
-                    const int4 u = *reinterpret_cast<const int4*>(sp + s * T + row0 + r);
-                    p[r] = u.x; p[r + 1] = u.y; p[r + 2] = u.z; p[r + 3] = u.w;
-                } else {
-                    p[r] = p[r + 1] = p[r + 2] = p[r + 3] = 0;
-                }
-            }
-            // Release the stage only once every lane's reads of it have
-            // landed: fold the loaded values, combine them across the warp
-            // (the reduction waits for each lane's loads), order the reads
-            // before the async-proxy (TMA) refill, and make the arrive's
-            // address depend on the combined value (through a run-time zero
-            // the compiler cannot fold away).
-            uint32_t dep = 0;
-#pragma unroll
-            for (int r = 0; r < R; ++r) dep ^= (uint32_t)k[r] ^ (uint32_t)p[r];
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
+            const uint32_t dep = round<R, Q, UNIQUE, ADD_BP, ADD_PP>(sk + s * T + row0, sp + s * T + row0,
+                                                                     (1u << R) - 1u, q, false, t, a);
+            // Release the stage once every lane's reads of it have landed:
+            // combine the values read across the warp (the reduction waits
+            // for each lane's loads), order the reads before the async-proxy
+            // (TMA) refill, and make the arrive's address depend on the
+            // combined value through a run-time zero the compiler cannot fold.
             const uint32_t wdep = __reduce_or_sync(0xffffffffu, dep);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             if (lane == 0) {
                 const uint32_t addr = smem_u32(&empty[s]) + ((wdep & zero) << 3);
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
             }
-            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
-            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(k, p, (1u << R) - 1u, q, false, t, a);
         }
         if (ok && blockIdx.x == gridDim.x - 1) {
             // rows of the last partial tile, straight from global memory
             const uint64_t base = nfull * T + (uint64_t)row0;
-            int32_t k[R], p[R];
             uint32_t valid = 0;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const bool in = base + r < n;
-                k[r] = in ? keys[base + r] : 0;
-                p[r] = (in && ADD_PP) ? pays[base + r] : 0;
-                valid |= (uint32_t)in << r;
-            }
+            for (int r = 0; r < R; ++r) valid |= (uint32_t)(base + 32 * r < n) << r;
             make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
-            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(k, p, valid, q, false, t, a);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false, t, a);
         }
         // drain the continuation queue
         make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, 0u);
     }
-    block_accumulate2<kThreads>(a.cnt, a.sum, acc);
+    block_accumulate2<kThreads>((unsigned long long)a.cnt, a.sum, acc);
 }
 
 template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
@@ -281,7 +274,8 @@ cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const
     auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP>;
     constexpr int T = kConsumerWarps * 32 * R;
     const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
-                        (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) + 2 * S * sizeof(uint64_t);
+                        (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) +
+                        kConsumerWarps * sizeof(uint32_t) + 2 * S * sizeof(uint64_t);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -320,8 +314,8 @@ cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, ui
     const mgv_tuning& tu = ctx->tuning;
     const int ctas = (int)tu.probe_ctas_per_sm;
     const int st = tu.probe_stages <= 2 ? 2 : tu.probe_stages <= 4 ? 4 : 6;
-    // Register budgets without spills on the unique-key path: R = 4 at 2 or
-    // 3 CTAs per SM (the latter when probe_ctas_per_sm asks for 3), R = 8 at 1.
+    // Register budgets: R = 4 at 2, 3 or 4 CTAs per SM (3 and 4 when
+    // probe_ctas_per_sm asks for them), R = 8 at 1.
 #define MGV_WS(RR, SS, MBB)                                                                        \
     return unique ? launch_mode<RR, SS, MBB, true>(keys, pays, n, t, mode, acc, ctas, s, ctx)     \
                   : launch_mode<RR, SS, MBB, false>(keys, pays, n, t, mode, acc, ctas, s, ctx)
@@ -337,6 +331,12 @@ cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, ui
             case 2: MGV_WS(4, 2, 3);
             case 4: MGV_WS(4, 4, 3);
             default: MGV_WS(4, 6, 3);
+        }
+    }
+    if (ctas == 4) {
+        switch (st) {
+            case 2: MGV_WS(4, 2, 4);
+            default: MGV_WS(4, 4, 4);
         }
     }
     switch (st) {

@@ -144,6 +144,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_gen_perm": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
         "mgv_gen_probe_keys": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint64, c_uint64, c_uint32,
                                     c_int64, c_uint64, POINTER(c_uint64), c_void_p]),
+        "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
         "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
     }
     for name, (res, args) in sigs.items():
@@ -220,6 +221,12 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def diag_random_gather(self, table_bytes: int, n: int, ctas_per_sm: int = 4, reps: int = 20) -> float:
+        """Milliseconds per pass of n random 32-byte bucket reads."""
+        ms = c_double()
+        _call("mgv_diag_random_gather", self.h, table_bytes, n, ctas_per_sm, reps, byref(ms))
+        return ms.value
 
     # seeded columns ---------------------------------------------------
     def gen_uniform(self, dst, n, seed, stream_id, lo, rng, stream=None):
