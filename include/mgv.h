@@ -272,6 +272,30 @@ mgv_status mgv_gen_probe_keys(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t s
 mgv_status mgv_gen_zipf(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint32_t stream_id,
                         uint32_t groups, double s, void *stream);
 
+/* ---- hash join without allocation ------------------------------------- */
+
+/* Largest build side mgv_hash_join_noalloc accepts. */
+#define MGV_NOALLOC_MAX_BUILD_ROWS (1u << 20)
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (code running under another framework's allocator or memory
+ * budget, inside a graph capture or real-time loop where an allocation would
+ * stall, or given only pre-allocated buffers): builds a hash table on the
+ * build columns and probes it with the probe columns, writing
+ * d_result[0] = COUNT(matches) and d_result[1] = SUM(build payload + probe
+ * payload) (int64, device memory) -- the result of
+ * create_count_join_1G_pipeline.  Needs no context and allocates nothing:
+ * the table lives in a fixed device array of MGV_NOALLOC_MAX_BUILD_ROWS rows
+ * (about 20 MiB, held by every GPU that loads the library until exit); a
+ * larger build side is rejected with MGV_EINVAL.  The first call on a device
+ * looks up the array's device address and should come before any stream
+ * capture.  All calls share the array and clear it first: calls that overlap
+ * on the GPU race.  Payload pointers may be NULL (payload 0).  Waits for
+ * `stream` before returning. */
+mgv_status mgv_hash_join_noalloc(int device, const int32_t *build_keys, const int32_t *build_payloads,
+                                 uint64_t build_rows, const int32_t *probe_keys, const int32_t *probe_payloads,
+                                 uint64_t probe_rows, int64_t *d_result, void *stream);
+
 /* ---- diagnostics ------------------------------------------------------ */
 
 /* Random 32-byte bucket-read ceiling: times `reps` passes of n hashed

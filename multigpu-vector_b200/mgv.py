@@ -144,6 +144,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_gen_perm": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
         "mgv_gen_probe_keys": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint64, c_uint64, c_uint32,
                                     c_int64, c_uint64, POINTER(c_uint64), c_void_p]),
+        "mgv_hash_join_noalloc": (st, [c_int, c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,
+                                       c_void_p, c_void_p]),
         "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
         "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
     }
@@ -374,6 +376,18 @@ class Op:
         if self.h:
             load().mgv_op_destroy(self.h)
             self.h = None
+
+
+NOALLOC_MAX_BUILD_ROWS = 1 << 20
+
+
+def hash_join_noalloc(device: int, build_keys, build_pay, build_rows: int, probe_keys, probe_pay, probe_rows: int,
+                      d_result, stream=None) -> None:
+    """mgv_hash_join_noalloc: COUNT + SUM(bp + pp) into d_result[0..1] (device int64),
+    using the library's fixed scratch table instead of allocating one."""
+    p = lambda x: c_void_p(0 if x is None else _ptr(x))
+    _call("mgv_hash_join_noalloc", device, p(build_keys), p(build_pay), build_rows, p(probe_keys), p(probe_pay),
+          probe_rows, p(d_result), _stream(stream))
 
 
 # ---- reference-style plans (src/main9.cu:202-367) ---------------------------
