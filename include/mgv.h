@@ -90,7 +90,8 @@ typedef struct mgv_tuning {
     uint32_t probe_ctas_per_sm;     /* 0 = as many as fit; 3 with 4 rows per thread
                                        selects the 3-CTA register budget               */
     float default_load_factor;      /* hash_build tables whose desc gives 0            */
-    uint32_t reserved[3];
+    uint32_t groupby_smem_slots;    /* per-CTA shared group table (power of 2, 0 = off) */
+    uint32_t reserved[2];
 } mgv_tuning;
 
 mgv_status mgv_ctx_set_tuning(mgv_ctx *ctx, const mgv_tuning *t);
@@ -176,13 +177,18 @@ typedef struct mgv_agg_result {
 
 /* hashjoin_builder (src/operators/hashjoin.cu:40-60), as an open-addressing
  * table of 32-byte buckets (4 {key, payload} slots, one L2 sector).
- * expected_rows sizes the table; load_factor in (0, 0.95] (0 = default
- * 0.5); payload_col -1 stores payload 0. */
+ * expected_rows sizes the table; load_factor in (0, 0.95] (0 = the context's
+ * default); payload_col -1 stores payload 0.  radix_bits > 0 lays the table
+ * out in 2^radix_bits regions, one per value of (key >> radix_shift) &
+ * (2^radix_bits - 1), so that a build fed partition by partition (by a
+ * partition operator with the same bits) touches one region at a time. */
 typedef struct mgv_hash_build_desc {
     uint32_t key_col;
     int32_t payload_col;
     uint64_t expected_rows;
     float load_factor;
+    uint32_t radix_bits;
+    uint32_t radix_shift;
     uint32_t reserved;
 } mgv_hash_build_desc;
 
@@ -213,8 +219,42 @@ typedef struct mgv_sink_desc {
     uint32_t reserved;
 } mgv_sink_desc;
 
+/* Hash GROUP BY (no reference counterpart; the reference has a global SUM
+ * only): int64 SUM(cols[value_col]) and COUNT(*) per distinct
+ * cols[group_col] (value_col -1: COUNT only; either may be `ncols`, the
+ * build payload appended by a hash_probe).  max_groups sizes the table. */
+typedef struct mgv_groupby_desc {
+    uint32_t group_col;
+    int32_t value_col;
+    uint32_t max_groups;
+    uint32_t reserved;
+} mgv_groupby_desc;
+
+typedef struct mgv_group_row {
+    int32_t group;
+    int32_t pad;
+    int64_t sum;
+    int64_t count;
+} mgv_group_row;
+
+/* split (src/operators/split.cu:49-118, partition by x & 1), generalised to
+ * 2^radix_bits partitions by (cols[key_col] >> radix_shift) & (2^bits - 1):
+ * the in-GPU exchange.  Rows are stored partition-major (capacity
+ * max_rows); close() pushes them, partition by partition, into the parent
+ * chain and then closes it. */
+typedef struct mgv_partition_desc {
+    uint32_t key_col;
+    uint32_t radix_bits;
+    uint32_t radix_shift;
+    uint32_t reserved;
+    uint64_t max_rows;
+} mgv_partition_desc;
+
 mgv_status mgv_op_create_select(mgv_ctx *ctx, const mgv_select_desc *desc, mgv_op *parent,
                                 mgv_op **out);
+mgv_status mgv_op_create_groupby(mgv_ctx *ctx, const mgv_groupby_desc *desc, mgv_op **out);
+mgv_status mgv_op_create_partition(mgv_ctx *ctx, const mgv_partition_desc *desc, mgv_op *parent,
+                                   mgv_op **out);
 mgv_status mgv_op_create_aggregate(mgv_ctx *ctx, const mgv_aggregate_desc *desc, mgv_op **out);
 mgv_status mgv_op_create_hash_build(mgv_ctx *ctx, const mgv_hash_build_desc *desc, mgv_op **out);
 mgv_status mgv_op_create_hash_probe(mgv_ctx *ctx, const mgv_hash_probe_desc *desc,
@@ -241,6 +281,8 @@ mgv_status mgv_op_close(mgv_op *op, void *stream);
  *   aggregate  -> mgv_agg_result
  *   hash_build -> mgv_hash_build_info
  *   sink       -> uint64_t row count
+ *   groupby    -> mgv_group_row[groups], sorted by group
+ *   partition  -> uint64_t[2^radix_bits] rows per partition
  * `needed` (may be NULL) receives the size in bytes. */
 mgv_status mgv_op_result(mgv_op *op, void *out, size_t bytes, size_t *needed);
 

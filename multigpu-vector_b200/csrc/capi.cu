@@ -71,6 +71,8 @@ static mgv_status check_device(Context* ctx, cudaStream_t s) {
     return report_device_error(ctx, w, s);
 }
 
+static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n, cudaStream_t s);
+
 extern "C" {
 
 const char* mgv_status_string(mgv_status s) {
@@ -399,16 +401,22 @@ mgv_status mgv_op_create_hash_build(mgv_ctx* ctx, const mgv_hash_build_desc* d, 
         return fail(MGV_EINVAL, "column out of range");
     float lf = d->load_factor == 0.0f ? ctx->tuning.default_load_factor : d->load_factor;
     if (!(lf > 0.0f && lf <= 0.95f)) return fail(MGV_EINVAL, "load_factor must be in (0, 0.95]");
+    if (d->radix_bits > 12 || d->radix_shift > 31) return fail(MGV_EINVAL, "radix_bits <= 12, radix_shift <= 31");
     const uint64_t rows = d->expected_rows ? d->expected_rows : 1;
-    const double nb = std::ceil((double)rows / (4.0 * lf));
-    if (nb >= 4294967295.0) return fail(MGV_EINVAL, "expected_rows too large");
+    const uint32_t parts = 1u << d->radix_bits;
+    // buckets per region: the expected rows of one region at the load factor
+    const double bpp = std::ceil((double)rows / parts / (4.0 * lf));
+    if (bpp * parts >= 4294967295.0) return fail(MGV_EINVAL, "expected_rows too large");
     MGV_CUDA_TRY(cudaSetDevice(ctx->device));
     mgv_op* o = new_op(ctx, OpKind::HashBuild);
     if (!o) return fail(MGV_ENOMEM, "host allocation");
     o->hb = *d;
     o->hb.load_factor = lf;
     TableView& t = o->table;
-    t.nbuckets = (uint32_t)std::max(1.0, nb);
+    t.bpp = (uint32_t)std::max(1.0, bpp);
+    t.radix_shift = d->radix_shift;
+    t.radix_mask = parts - 1;
+    t.nbuckets = t.bpp * parts;
     t.side_cap = rows;
     o->table_bytes = (size_t)t.nbuckets * 32;
     mgv_status st = dev_alloc(o, (void**)&t.slots, o->table_bytes);
@@ -433,6 +441,53 @@ mgv_status mgv_op_create_hash_probe(mgv_ctx* ctx, const mgv_hash_probe_desc* d, 
     if (!o) return fail(MGV_ENOMEM, "host allocation");
     o->hp = *d;
     o->parent = parent;
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_groupby(mgv_ctx* ctx, const mgv_groupby_desc* d, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (d->group_col > MGV_MAX_COLS || d->value_col < -1 || d->value_col > MGV_MAX_COLS)
+        return fail(MGV_EINVAL, "column out of range");
+    if (d->max_groups == 0 || d->max_groups > (1u << 30)) return fail(MGV_EINVAL, "max_groups out of range");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_op* o = new_op(ctx, OpKind::Groupby);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->gb = *d;
+    uint32_t cap = 1024;
+    while (cap < 2u * d->max_groups) cap <<= 1;
+    GroupTableView& g = o->gtab;
+    g.cap = cap;
+    mgv_status st = dev_alloc(o, (void**)&g.keys, sizeof(int32_t) * cap);
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&g.sums, sizeof(unsigned long long) * cap);
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&g.counts, sizeof(unsigned long long) * cap);
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&g.special, 2 * sizeof(unsigned long long));
+    if (st != MGV_OK) {
+        for (void* p : o->allocs) cudaFree(p);
+        delete o;
+        return st;
+    }
+    *out = o;
+    return MGV_OK;
+}
+
+mgv_status mgv_op_create_partition(mgv_ctx* ctx, const mgv_partition_desc* d, mgv_op* parent, mgv_op** out) {
+    if (!ctx || !d || !out) return fail(MGV_EINVAL, "NULL argument");
+    if (!parent) return fail(MGV_EINVAL, "partition needs a parent");
+    if (d->key_col >= MGV_MAX_COLS) return fail(MGV_EINVAL, "key column out of range");
+    if (d->radix_bits < 1 || d->radix_bits > 12 || d->radix_shift > 31)
+        return fail(MGV_EINVAL, "radix_bits must be in [1, 12], radix_shift <= 31");
+    if (d->max_rows == 0) return fail(MGV_EINVAL, "max_rows must be > 0");
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_op* o = new_op(ctx, OpKind::Partition);
+    if (!o) return fail(MGV_ENOMEM, "host allocation");
+    o->pt = *d;
+    o->parent = parent;
+    mgv_status st = dev_alloc(o, (void**)&o->pt_dev, sizeof(unsigned long long) << d->radix_bits);
+    if (st != MGV_OK) {
+        delete o;
+        return st;
+    }
     *out = o;
     return MGV_OK;
 }
@@ -508,6 +563,18 @@ static mgv_status op_reset(Op* o, cudaStream_t s) {
             if (o->hp.build->state != OpState::Closed)
                 return fail(MGV_ESTATE, "hash_probe opened before its build side was closed");
             break;
+        case OpKind::Groupby:
+            MGV_CUDA_TRY(launch_fill_i32(o->gtab.keys, o->gtab.cap, kEmptyKey, s, o->ctx));
+            MGV_CUDA_TRY(cudaMemsetAsync(o->gtab.sums, 0, sizeof(unsigned long long) * o->gtab.cap, s));
+            MGV_CUDA_TRY(cudaMemsetAsync(o->gtab.counts, 0, sizeof(unsigned long long) * o->gtab.cap, s));
+            MGV_CUDA_TRY(cudaMemsetAsync(o->gtab.special, 0, 2 * sizeof(unsigned long long), s));
+            o->gb_rows.clear();
+            break;
+        case OpKind::Partition:
+            o->pt_fill = 0;
+            o->pt_runs.clear();
+            o->pt_hist.assign((size_t)1 << o->pt.radix_bits, 0);
+            break;
         default: break;
     }
     return MGV_OK;
@@ -552,6 +619,24 @@ static mgv_status op_finish(Op* o, cudaStream_t s) {
             o->unique = m[3] == 0;
             break;
         }
+        case OpKind::Groupby: {
+            const uint32_t cap = o->gtab.cap;
+            std::vector<int32_t> keys(cap);
+            std::vector<unsigned long long> sums(cap), counts(cap), special(2);
+            MGV_CUDA_TRY(cudaMemcpyAsync(keys.data(), o->gtab.keys, sizeof(int32_t) * cap, cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(sums.data(), o->gtab.sums, 8ull * cap, cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(counts.data(), o->gtab.counts, 8ull * cap, cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(special.data(), o->gtab.special, 16, cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            o->gb_rows.clear();
+            if (special[1]) o->gb_rows.push_back(mgv_group_row{kEmptyKey, 0, (int64_t)special[0], (int64_t)special[1]});
+            for (uint32_t i = 0; i < cap; ++i)
+                if (keys[i] != kEmptyKey && counts[i])
+                    o->gb_rows.push_back(mgv_group_row{keys[i], 0, (int64_t)sums[i], (int64_t)counts[i]});
+            std::sort(o->gb_rows.begin(), o->gb_rows.end(),
+                      [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+            break;
+        }
         case OpKind::Sink: {
             unsigned long long rows = 0;
             MGV_CUDA_TRY(cudaMemcpyAsync(&rows, o->sink.cursor, sizeof(rows), cudaMemcpyDeviceToHost, s));
@@ -594,7 +679,17 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
         if (st == MGV_OK) st = st2;
         return st;
     }
-    return mgv_op_close(static_cast<mgv_op*>(o->parent), stream);  // after_close
+    if (o->kind == OpKind::Partition) {
+        // push the stored rows, partition by partition, into the parent chain
+        for (const auto& run : o->pt_runs) {
+            const int32_t* cols[MGV_MAX_COLS];
+            for (uint32_t c = 0; c < o->pt_ncols; ++c) cols[c] = o->pt_store + c * o->pt.max_rows + run.first;
+            st = consume_cols(o->parent, cols, o->pt_ncols, run.second, s);
+            if (st != MGV_OK) break;
+        }
+    }
+    mgv_status st2 = mgv_op_close(static_cast<mgv_op*>(o->parent), stream);  // after_close
+    return st != MGV_OK ? st : st2;
 }
 
 mgv_status mgv_op_result(mgv_op* o, void* out, size_t bytes, size_t* needed) {
@@ -606,6 +701,8 @@ mgv_status mgv_op_result(mgv_op* o, void* out, size_t bytes, size_t* needed) {
         case OpKind::Aggregate: src = &o->agg_result; n = sizeof(o->agg_result); break;
         case OpKind::HashBuild: src = &o->hb_info; n = sizeof(o->hb_info); break;
         case OpKind::Sink: src = &o->sink_rows; n = sizeof(o->sink_rows); break;
+        case OpKind::Groupby: src = o->gb_rows.data(); n = o->gb_rows.size() * sizeof(mgv_group_row); break;
+        case OpKind::Partition: src = o->pt_hist.data(); n = o->pt_hist.size() * sizeof(uint64_t); break;
         default: return fail(MGV_EINVAL, "operator has no result");
     }
     if (needed) *needed = n;
@@ -644,8 +741,48 @@ static bool all_open(Op* o) {
     return true;
 }
 
-static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n,
-                               cudaStream_t s) {
+}  // extern "C"
+
+// Partition consume: histogram, prefix sums, scatter into the op's store.
+static mgv_status consume_partition(Op* part, Op* sel, const int32_t* const* cols, uint32_t ncols, uint64_t n,
+                                    cudaStream_t s) {
+    Context* ctx = part->ctx;
+    const uint32_t P = 1u << part->pt.radix_bits;
+    if (part->pt_store == nullptr) {
+        part->pt_ncols = ncols;
+        mgv_status st = dev_alloc(part, (void**)&part->pt_store, sizeof(int32_t) * ncols * part->pt.max_rows);
+        if (st != MGV_OK) return st;
+    }
+    if (ncols != part->pt_ncols) return fail(MGV_EINVAL, "partition: every consume must carry the same columns");
+    if (n == 0) return MGV_OK;
+    MGV_CUDA_TRY(cudaMemsetAsync(part->pt_dev, 0, sizeof(unsigned long long) * P, s));
+    MGV_CUDA_TRY(launch_partition_hist(cols, n, sel != nullptr, sel ? sel->sel.col : 0, sel ? sel->sel.bound : 0,
+                                       part->pt.key_col, part->pt.radix_shift, part->pt.radix_bits, part->pt_dev, s,
+                                       ctx));
+    std::vector<unsigned long long> hist(P);
+    MGV_CUDA_TRY(cudaMemcpyAsync(hist.data(), part->pt_dev, 8ull * P, cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+    uint64_t rows = 0;
+    std::vector<unsigned long long> cursor(P);
+    for (uint32_t p = 0; p < P; ++p) {
+        cursor[p] = part->pt_fill + rows;
+        rows += hist[p];
+        part->pt_hist[p] += hist[p];
+    }
+    if (part->pt_fill + rows > part->pt.max_rows)
+        return fail(MGV_ENOMEM, "partition: more rows than max_rows");
+    MGV_CUDA_TRY(cudaMemcpyAsync(part->pt_dev, cursor.data(), 8ull * P, cudaMemcpyHostToDevice, s));
+    MGV_CUDA_TRY(launch_partition_scatter(cols, ncols, n, sel != nullptr, sel ? sel->sel.col : 0,
+                                          sel ? sel->sel.bound : 0, part->pt.key_col, part->pt.radix_shift,
+                                          part->pt.radix_bits, part->pt_dev, part->pt_store, part->pt.max_rows, s,
+                                          ctx));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));  // the host cursors above must outlive the copy
+    if (rows) part->pt_runs.emplace_back(part->pt_fill, rows);
+    part->pt_fill += rows;
+    return MGV_OK;
+}
+
+static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n, cudaStream_t s) {
     Context* ctx = head->ctx;
     Op* sel = nullptr;
     Op* probe = nullptr;
@@ -653,70 +790,104 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
     if (o->kind == OpKind::Select) { sel = o; o = o->parent; }
     if (o && o->kind == OpKind::HashProbe) { probe = o; o = o->parent; }
     Op* term = o;
-    if (!term || term->parent) return fail(MGV_EUNSUPPORTED, "chain must be [select] [hash_probe] terminal");
+    if (!term || (term->parent && term->kind != OpKind::Partition))
+        return fail(MGV_EUNSUPPORTED, "chain must be [select] [hash_probe] terminal");
     auto col_ok = [&](int32_t c) { return c >= 0 && (uint32_t)c < ncols; };
+    // a column of the chain's rows: an input column, or the build payload (ncols)
+    auto ref_ok = [&](int32_t c) { return c == -1 || col_ok(c) || (probe && (uint32_t)c == ncols); };
     if (sel && !col_ok((int32_t)sel->sel.col)) return fail(MGV_EINVAL, "select column not in input");
     if (probe && !col_ok((int32_t)probe->hp.key_col)) return fail(MGV_EINVAL, "probe key column not in input");
-    if (n == 0) return MGV_OK;
+
+    ChainArgs a{};
+    for (uint32_t c = 0; c < ncols; ++c) a.cols[c] = cols[c];
+    a.ncols = ncols;
+    a.n = n;
+    a.has_sel = sel != nullptr;
+    if (sel) { a.sel_col = sel->sel.col; a.sel_bound = sel->sel.bound; }
+    a.has_probe = probe != nullptr;
+    if (probe) {
+        a.probe_col = probe->hp.key_col;
+        a.table = probe->hp.build->table;
+        a.unique = probe->hp.build->unique;
+    }
 
     switch (term->kind) {
         case OpKind::Aggregate: {
-            const int32_t a = term->agg.sum_col_a, b = term->agg.sum_col_b;
+            const int32_t ca = term->agg.sum_col_a, cb = term->agg.sum_col_b;
+            if (!ref_ok(ca) || !ref_ok(cb)) return fail(MGV_EINVAL, "aggregate column not in input");
+            if (n == 0) return MGV_OK;
             if (!probe) {
-                if ((a != -1 && !col_ok(a)) || (b != -1 && !col_ok(b)))
-                    return fail(MGV_EINVAL, "aggregate column not in input");
                 MGV_CUDA_TRY(launch_select_agg(sel ? cols[sel->sel.col] : nullptr, sel ? sel->sel.bound : 0,
-                                               sel != nullptr, a >= 0 ? cols[a] : nullptr,
-                                               b >= 0 ? cols[b] : nullptr, n, term->d_acc, s, ctx));
+                                               sel != nullptr, ca >= 0 ? cols[ca] : nullptr,
+                                               cb >= 0 ? cols[cb] : nullptr, n, term->d_acc, s, ctx));
                 return MGV_OK;
             }
-            if (sel) return fail(MGV_EUNSUPPORTED, "select -> hash_probe -> aggregate is not fused yet");
-            // columns: input 0..ncols-1, build payload = ncols
-            uint32_t mode = 0;
-            const int32_t* pays = nullptr;
-            for (int32_t c : {a, b}) {
-                if (c == -1) continue;
-                if ((uint32_t)c == ncols) { mode |= 1u; continue; }
-                if (!col_ok(c)) return fail(MGV_EINVAL, "aggregate column not in input");
-                if (pays) return fail(MGV_EUNSUPPORTED, "probe aggregate sums at most one probe column");
-                pays = cols[c];
-                mode |= 2u;
+            // probe -> aggregate without a select: the warp-specialised probe
+            // (sums the build payload and at most one probe column)
+            if (!sel && !(ca >= 0 && cb >= 0 && ca != (int32_t)ncols && cb != (int32_t)ncols)) {
+                uint32_t mode = 0;
+                const int32_t* pays = nullptr;
+                for (int32_t c : {ca, cb}) {
+                    if (c == -1) continue;
+                    if ((uint32_t)c == ncols) mode |= 1u;
+                    else { pays = cols[c]; mode |= 2u; }
+                }
+                Op* hb = probe->hp.build;
+                MGV_CUDA_TRY(launch_probe_agg(cols[probe->hp.key_col], pays, n, hb->table, hb->unique, mode,
+                                              term->d_acc, s, ctx));
+                return MGV_OK;
             }
-            Op* hb = probe->hp.build;
-            MGV_CUDA_TRY(launch_probe_agg(cols[probe->hp.key_col], pays, n, hb->table, hb->unique, mode,
-                                          term->d_acc, s, ctx));
+            a.term = kTermAgg;
+            a.ref[0] = ca;
+            a.ref[1] = cb;
+            a.nref = 2;
+            a.acc = term->d_acc;
+            MGV_CUDA_TRY(launch_chain(a, s, ctx));
+            return MGV_OK;
+        }
+        case OpKind::Groupby: {
+            const int32_t g = (int32_t)term->gb.group_col, v = term->gb.value_col;
+            if (!ref_ok(g) || g == -1 || !ref_ok(v)) return fail(MGV_EINVAL, "group-by column not in input");
+            if (n == 0) return MGV_OK;
+            a.term = kTermGroupby;
+            a.ref[0] = g;
+            a.ref[1] = v;
+            a.nref = 2;
+            a.gt = term->gtab;
+            a.smem_groups = ctx->tuning.groupby_smem_slots;
+            MGV_CUDA_TRY(launch_chain(a, s, ctx));
+            return MGV_OK;
+        }
+        case OpKind::Sink: {
+            if (n == 0) return MGV_OK;
+            const uint32_t out_cols = std::min(ncols + (probe ? 1u : 0u), term->sink.pool_ncols);
+            a.term = kTermSink;
+            a.nref = out_cols;
+            for (uint32_t c = 0; c < out_cols; ++c) a.ref[c] = (int32_t)c;
+            a.sink = term->sink;
+            a.sink.ncols = out_cols;
+            MGV_CUDA_TRY(launch_chain(a, s, ctx));
             return MGV_OK;
         }
         case OpKind::HashBuild: {
             if (probe) return fail(MGV_EUNSUPPORTED, "hash_probe cannot feed hash_build");
             const int32_t kc = (int32_t)term->hb.key_col, pc = term->hb.payload_col;
             if (!col_ok(kc) || (pc != -1 && !col_ok(pc))) return fail(MGV_EINVAL, "build column not in input");
+            if (n == 0) return MGV_OK;
             MGV_CUDA_TRY(launch_build(cols[kc], pc >= 0 ? cols[pc] : nullptr, sel ? cols[sel->sel.col] : nullptr,
                                       sel ? sel->sel.bound : 0, sel != nullptr, n, term->table, s, ctx));
             return MGV_OK;
         }
-        case OpKind::Sink: {
-            ChainArgs a{};
-            for (uint32_t c = 0; c < ncols; ++c) a.cols[c] = cols[c];
-            a.ncols = ncols;
-            a.n = n;
-            a.has_sel = sel != nullptr;
-            if (sel) { a.sel_col = sel->sel.col; a.sel_bound = sel->sel.bound; }
-            a.has_probe = probe != nullptr;
-            if (probe) {
-                a.probe_col = probe->hp.key_col;
-                a.table = probe->hp.build->table;
-                a.unique = probe->hp.build->unique;
-            }
-            const uint32_t out_cols = ncols + (probe ? 1u : 0u);
-            SinkView sv = term->sink;
-            sv.ncols = std::min(out_cols, term->sink.pool_ncols);
-            MGV_CUDA_TRY(launch_chain_sink(a, sv, s, ctx));
-            return MGV_OK;
+        case OpKind::Partition: {
+            if (probe) return fail(MGV_EUNSUPPORTED, "hash_probe cannot feed a partition");
+            if (!col_ok((int32_t)term->pt.key_col)) return fail(MGV_EINVAL, "partition key column not in input");
+            return consume_partition(term, sel, cols, ncols, n, s);
         }
         default: return fail(MGV_EUNSUPPORTED, "no kernel for this chain");
     }
 }
+
+extern "C" {
 
 mgv_status mgv_op_consume_columns(mgv_op* o, const int32_t* const* cols, uint32_t ncols, uint64_t rows,
                                   void* stream) {

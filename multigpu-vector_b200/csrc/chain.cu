@@ -1,0 +1,431 @@
+// chain.cu -- the generic fused operator chain:
+//
+//     [select] -> [hash_probe] -> { aggregate | group-by | sink }
+//
+// one kernel per consume call.  Warp-ballot select as in
+// unstable_select::consume_warp (src/operators/select3.cu:19-85): each warp
+// takes 128-row windows, evaluates the predicate and compacts the qualifying
+// rows with __ballot_sync / __popc into a per-warp shared-memory ring of 256
+// rows, carrying only the columns the rest of the chain reads (the others
+// are never loaded).  Full 128-row vectors then go through the probe and the
+// terminal (the reference's parent->consume_warp(x, 128)).
+//
+// The probe emits one output row per matching build row (all duplicates
+// match, src/operators/hashjoin.cu:148-162); the build payload of the match
+// is visible to the terminal as column `ncols`.
+//
+// Group-by (no reference counterpart): each CTA aggregates into a
+// shared-memory hash table; rows of equal group within a warp are first
+// combined with __match_any_sync + __reduce_add_sync, so a hot (Zipf) group
+// costs one shared atomic per warp instead of one per row.  Groups that do
+// not find a shared slot within a few probes go to the global table; at the
+// end of the CTA the shared table is merged into the global one.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "hash_table.cuh"
+#include "mgv_internal.h"
+
+namespace mgv {
+
+constexpr int kChainBlock = 256;
+constexpr int kChainWarps = kChainBlock / 32;
+constexpr int kRing = 256;
+
+struct ChainDev {
+    const int32_t* cols[MGV_MAX_COLS];
+    uint64_t n;
+    uint32_t ncols;
+    uint32_t nslots;                 // carried columns
+    int32_t slot_src[MGV_MAX_COLS];  // input column of each carried slot
+    uint32_t sel_col;
+    int32_t sel_bound;
+    int32_t probe_slot;
+    TableView table;
+    // terminal column references: carried slot, kBP (build payload) or -1
+    int32_t ref[MGV_MAX_COLS + 2];
+    uint32_t nref;
+    unsigned long long* acc;
+    GroupTableView gt;
+    uint32_t smem_groups;  // power of two, 0 = no shared table
+    SinkView sink;
+};
+
+constexpr int32_t kBP = 100;  // reference to the build payload
+
+// ---- device buffer pool: pop (swap-on-full for the sink) -------------------
+
+__device__ __forceinline__ uint32_t pool_pop(PoolDev* p, uint32_t tries) {
+    for (uint32_t i = 0; i < tries; ++i) {
+        unsigned long long h = atomicAdd(&p->head, 0ull);
+        uint32_t top = (uint32_t)h;
+        if (top == kNil) return kNil;
+        uint32_t nxt = *((volatile uint32_t*)&p->next[top]);
+        unsigned long long nh = (((h >> 32) + 1ull) << 32) | nxt;
+        if (atomicCAS(&p->head, h, nh) == h) {
+            atomicSub(&p->available, 1u);
+            return top;
+        }
+    }
+    return kNil;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Buffer id for chunk c of a sink; the warp that owns row c*capacity takes
+// a buffer from the pool and publishes it, everyone else waits for it with
+// a bounded wait (swap-on-full, src/buffer_manager.cuh:147-176).
+__device__ uint32_t sink_chunk(const SinkView& s, uint32_t c, bool opener, uint32_t* err) {
+    if (opener) {
+        uint32_t id = pool_pop(s.pool, 4096);
+        if (id == kNil) {
+            set_error(err, kDevOverflow, 3);
+            id = kNil - 1;  // published "no buffer" marker
+        }
+        atomicExch(s.chain + c, id);
+        return id;
+    }
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        uint32_t id = *((volatile uint32_t*)(s.chain + c));
+        if (id != kNil) return id;
+        if (global_ns() - t0 > 2000000000ull) {  // 2 s
+            set_error(err, kDevTimeout, 4);
+            return kNil - 1;
+        }
+        __nanosleep(64);
+    }
+}
+
+// Append `my_cnt` rows per lane, reserved warp-wide; row_val(i, col).
+template <class RowFn>
+__device__ __forceinline__ void sink_emit_warp(const SinkView& s, uint32_t my_cnt, RowFn row_val, uint32_t* err) {
+    const uint32_t lane = lane_id();
+    uint32_t incl = my_cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(s.cursor, (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned long long limit = (unsigned long long)s.max_chunks * s.capacity;
+    const unsigned long long first_c = base / s.capacity;
+    const unsigned long long last_c = (base + total - 1) / s.capacity;
+    uint32_t my_chunk_id = kNil - 1;
+    const unsigned long long c = first_c + lane;
+    if (c <= last_c && c < s.max_chunks) {
+        const bool opener = c * s.capacity >= base;  // this warp owns the chunk's first row
+        my_chunk_id = sink_chunk(s, (uint32_t)c, opener, err);
+    }
+    __syncwarp();
+    if (lane == 0 && (last_c - first_c >= 32 || base + total > limit)) set_error(err, kDevOverflow, 5);
+    const uint32_t maxc = __reduce_max_sync(0xffffffffu, my_cnt);
+    const unsigned long long pos0 = base + incl - my_cnt;
+    for (uint32_t i = 0; i < maxc; ++i) {
+        const bool act = i < my_cnt;
+        const unsigned long long pos = pos0 + i;
+        const unsigned long long rel = act ? pos / s.capacity - first_c : 0ull;
+        const uint32_t id = __shfl_sync(0xffffffffu, my_chunk_id, (int)(rel & 31ull));
+        if (!act || pos >= limit || rel >= 32 || id >= s.pool->nbuffers) continue;
+        const uint32_t off = (uint32_t)(pos % s.capacity);
+        int32_t* base_ptr = s.slab + (size_t)id * s.pool_ncols * s.capacity;
+        for (uint32_t col = 0; col < s.ncols; ++col) base_ptr[(size_t)col * s.capacity + off] = row_val(i, col);
+    }
+}
+
+// ---- group tables ------------------------------------------------------------
+
+__device__ __forceinline__ void global_group_add(const GroupTableView& gt, int32_t g, unsigned long long sum,
+                                                 unsigned long long cnt, uint32_t* err) {
+    if (g == kEmptyKey) {  // the reserved key has its own counters
+        atomicAdd(gt.special + 0, sum);
+        atomicAdd(gt.special + 1, cnt);
+        return;
+    }
+    uint32_t slot = murmur32((uint32_t)g) & (gt.cap - 1);
+    for (uint32_t i = 0; i < gt.cap; ++i) {
+        int32_t k = *((volatile int32_t*)(gt.keys + slot));
+        if (k == kEmptyKey) k = atomicCAS(gt.keys + slot, kEmptyKey, g);
+        if (k == kEmptyKey || k == g) {
+            atomicAdd(gt.sums + slot, sum);
+            atomicAdd(gt.counts + slot, cnt);
+            return;
+        }
+        slot = (slot + 1) & (gt.cap - 1);
+    }
+    set_error(err, kDevTableFull, 20);
+}
+
+struct SmemGroups {
+    int32_t* keys;
+    unsigned long long* sums;
+    uint32_t* counts;
+    uint32_t cap;  // 0 = no shared table
+};
+
+__device__ __forceinline__ void group_insert(const SmemGroups& sg, const GroupTableView& gt, int32_t g, long long sum,
+                                             uint32_t cnt, uint32_t* err) {
+    if (sg.cap && g != kEmptyKey) {
+        uint32_t slot = murmur32((uint32_t)g) & (sg.cap - 1);
+#pragma unroll 1
+        for (int i = 0; i < 8; ++i) {
+            int32_t k = sg.keys[slot];
+            if (k == kEmptyKey) k = atomicCAS(sg.keys + slot, kEmptyKey, g);
+            if (k == kEmptyKey || k == g) {
+                atomicAdd(sg.sums + slot, (unsigned long long)sum);
+                atomicAdd(sg.counts + slot, cnt);
+                return;
+            }
+            slot = (slot + 1) & (sg.cap - 1);
+        }
+    }
+    global_group_add(gt, g, (unsigned long long)sum, cnt, err);
+}
+
+// Warp-collective: add (g, v) for every active lane.  Lanes with the same
+// group are combined first; the sum of up to 32 int32 values is exact from
+// two 16-bit halves (each half-sum stays below 2^21).
+__device__ __forceinline__ void group_add_warp(bool active, int32_t g, int32_t v, const SmemGroups& sg,
+                                               const GroupTableView& gt, uint32_t* err) {
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (!act || !active) return;
+    const unsigned peers = __match_any_sync(act, g);
+    const uint32_t lo = (uint32_t)v & 0xffffu;
+    const uint32_t hi = (uint32_t)((v >> 16) + 32768);
+    const uint32_t slo = __reduce_add_sync(peers, lo);
+    const uint32_t shi = __reduce_add_sync(peers, hi);
+    if ((int)lane_id() == __ffs(peers) - 1) {
+        const uint32_t c = __popc(peers);
+        const long long sum = ((long long)shi - 32768ll * c) * 65536ll + (long long)slo;
+        group_insert(sg, gt, g, sum, c, err);
+    }
+}
+
+// ---- the chain kernel ----------------------------------------------------------
+
+template <bool SEL, bool PROBE, bool UNIQUE, int TERM>
+__global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t warp = threadIdx.x / 32, lane = lane_id();
+    // shared layout: [group sums u64 | ring int32 | group keys int32 | group counts u32]
+    SmemGroups sg{nullptr, nullptr, nullptr, 0};
+    unsigned long long* gsums = reinterpret_cast<unsigned long long*>(smem_raw);
+    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + (TERM == kTermGroupby ? a.smem_groups * 8 : 0));
+    if (TERM == kTermGroupby && a.smem_groups) {
+        sg.sums = gsums;
+        sg.keys = rings + kChainWarps * a.nslots * kRing;
+        sg.counts = reinterpret_cast<uint32_t*>(sg.keys + a.smem_groups);
+        sg.cap = a.smem_groups;
+        for (uint32_t i = threadIdx.x; i < sg.cap; i += kChainBlock) {
+            sg.keys[i] = kEmptyKey;
+            sg.sums[i] = 0;
+            sg.counts[i] = 0;
+        }
+        __syncthreads();
+    }
+    int32_t* ring = rings + (size_t)warp * a.nslots * kRing;
+    unsigned long long acnt = 0, asum = 0;
+
+    // value of terminal reference r for ring row rp and build payload bp
+    auto val = [&](int32_t ref, uint32_t rp, int32_t bp) -> int32_t {
+        return ref == kBP ? bp : ring[ref * kRing + rp];
+    };
+    // one output row (warp-collective)
+    auto emit = [&](bool active, uint32_t rp, int32_t bp) {
+        if (TERM == kTermAgg) {
+            if (active) {
+                long long t = 0;
+                if (a.ref[0] >= 0) t += val(a.ref[0], rp, bp);
+                if (a.ref[1] >= 0) t += val(a.ref[1], rp, bp);
+                acnt += 1;
+                asum += (unsigned long long)t;
+            }
+        } else if (TERM == kTermGroupby) {
+            const int32_t g = active ? val(a.ref[0], rp, bp) : 0;
+            const int32_t v = (active && a.ref[1] >= 0) ? val(a.ref[1], rp, bp) : 0;
+            group_add_warp(active, g, v, sg, a.gt, err);
+        } else {
+            sink_emit_warp(
+                a.sink, active ? 1u : 0u, [&](uint32_t, uint32_t col) { return val(a.ref[col], rp, bp); }, err);
+        }
+    };
+
+    // push `cnt` (<= 128) dense ring rows starting at `start`
+    auto push_vector = [&](uint32_t start, uint32_t cnt) {
+        __syncwarp();
+        if (!PROBE) {
+#pragma unroll 1
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t idx = j * 32 + lane;
+                emit(idx < cnt, (start + idx) & (kRing - 1), 0);
+            }
+        } else {
+            // home-bucket loads of all four rows first, then walk each run
+            uint32_t w[4][8];
+            uint32_t hb[4];
+            int32_t key[4];
+            bool in[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t idx = j * 32 + lane;
+                in[j] = idx < cnt;
+                key[j] = in[j] ? ring[a.probe_slot * kRing + ((start + idx) & (kRing - 1))] : 0;
+                hb[j] = home_bucket(key[j], a.table);
+                if (in[j] && key[j] != kEmptyKey) ld_bucket(a.table.slots + 4ull * hb[j], w[j]);
+            }
+            const uint32_t side_n =
+                (uint32_t)min((unsigned long long)a.table.meta[0], (unsigned long long)a.table.side_cap);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t rp = (start + j * 32 + lane) & (kRing - 1);
+                uint32_t wb[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wb[q] = w[j][q];
+                uint32_t b = hb[j], slot = 0, side_i = 0;
+                const bool reserved = in[j] && key[j] == kEmptyKey;
+                bool done = !in[j] || reserved;
+                bool side_done = !reserved;
+                for (uint32_t guard = 0;; ++guard) {
+                    const bool more_any = __any_sync(0xffffffffu, !done || !side_done);
+                    if (!more_any || guard > a.table.nbuckets * 5u + side_n + 8u) break;
+                    bool found = false;
+                    int32_t bp = 0;
+                    if (!side_done) {
+                        if (side_i < side_n) {
+                            found = true;
+                            bp = a.table.side_pay[side_i++];
+                        }
+                        if (side_i >= side_n) side_done = true;
+                    } else if (!done) {
+#pragma unroll
+                        for (uint32_t q = 0; q < 4; ++q) {
+                            if (!found && q >= slot && wb[2 * q] == (uint32_t)key[j]) {
+                                found = true;
+                                bp = (int32_t)wb[2 * q + 1];
+                                slot = q + 1;
+                            }
+                        }
+                        if (found) {
+                            if (UNIQUE) done = true;
+                        } else if (wb[6] != (uint32_t)kEmptyKey) {  // run continues
+                            b = (b + 1 == a.table.nbuckets) ? 0u : b + 1;
+                            slot = 0;
+                            ld_bucket(a.table.slots + 4ull * b, wb);
+                        } else {
+                            done = true;
+                        }
+                    }
+                    emit(found, rp, bp);
+                }
+            }
+        }
+        __syncwarp();
+    };
+
+    const uint64_t nwin = (a.n + 127) / 128;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * kChainWarps + warp;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kChainWarps;
+    uint32_t head = 0, fill = 0;
+    for (uint64_t win = gwarp; win < nwin; win += nwarps) {
+        const uint64_t r0 = win * 128;
+#pragma unroll 1
+        for (int j = 0; j < 4; ++j) {
+            const uint64_t row = r0 + j * 32 + lane;
+            bool pass = row < a.n;
+            if (SEL && pass) pass = __ldg(a.cols[a.sel_col] + row) <= a.sel_bound;
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) {
+                const uint32_t pos = (head + fill + __popc(m & ((1u << lane) - 1u))) & (kRing - 1);
+                for (uint32_t c = 0; c < a.nslots; ++c) ring[c * kRing + pos] = __ldg(a.cols[a.slot_src[c]] + row);
+            }
+            fill += __popc(m);
+            if (fill >= 128) {
+                push_vector(head, 128);
+                head = (head + 128) & (kRing - 1);
+                fill -= 128;
+            }
+        }
+    }
+    if (fill) push_vector(head, fill);
+
+    if (TERM == kTermAgg) block_accumulate2<kChainBlock>(acnt, asum, a.acc);
+    if (TERM == kTermGroupby && a.smem_groups) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < sg.cap; i += kChainBlock)
+            if (sg.keys[i] != kEmptyKey && sg.counts[i]) global_group_add(a.gt, sg.keys[i], sg.sums[i], sg.counts[i], err);
+    }
+}
+
+template <bool SEL, bool PROBE, bool UNIQUE, int TERM>
+static cudaError_t launch_chain_t(const ChainDev& d, size_t smem, uint64_t n, cudaStream_t s, Context* ctx) {
+    auto k = k_chain<SEL, PROBE, UNIQUE, TERM>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int grid = occupancy_grid((const void*)k, kChainBlock, smem, ctx);
+    const uint64_t need = ((n + 127) / 128 + kChainWarps - 1) / kChainWarps;
+    if ((uint64_t)grid > need) grid = (int)(need ? need : 1);
+    k<<<grid, kChainBlock, smem, s>>>(d, ctx->d_err);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+template <int TERM>
+static cudaError_t launch_chain_term(const ChainArgs& a, const ChainDev& d, size_t smem, cudaStream_t s, Context* ctx) {
+    if (!a.has_probe)
+        return a.has_sel ? launch_chain_t<true, false, false, TERM>(d, smem, a.n, s, ctx)
+                         : launch_chain_t<false, false, false, TERM>(d, smem, a.n, s, ctx);
+    if (a.unique)
+        return a.has_sel ? launch_chain_t<true, true, true, TERM>(d, smem, a.n, s, ctx)
+                         : launch_chain_t<false, true, true, TERM>(d, smem, a.n, s, ctx);
+    return a.has_sel ? launch_chain_t<true, true, false, TERM>(d, smem, a.n, s, ctx)
+                     : launch_chain_t<false, true, false, TERM>(d, smem, a.n, s, ctx);
+}
+
+cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx) {
+    if (a.n == 0) return cudaSuccess;
+    ChainDev d{};
+    for (uint32_t c = 0; c < a.ncols; ++c) d.cols[c] = a.cols[c];
+    d.n = a.n;
+    d.ncols = a.ncols;
+    d.sel_col = a.sel_col;
+    d.sel_bound = a.sel_bound;
+    d.table = a.table;
+    d.acc = a.acc;
+    d.gt = a.gt;
+    d.sink = a.sink;
+    // carried columns: the probe key and every column the terminal reads
+    int32_t slot_of[MGV_MAX_COLS];
+    for (int c = 0; c < MGV_MAX_COLS; ++c) slot_of[c] = -1;
+    auto carry = [&](int32_t col) -> int32_t {
+        if (col < 0) return -1;
+        if ((uint32_t)col == a.ncols) return kBP;
+        if (slot_of[col] < 0) {
+            slot_of[col] = (int32_t)d.nslots;
+            d.slot_src[d.nslots++] = col;
+        }
+        return slot_of[col];
+    };
+    d.probe_slot = a.has_probe ? carry((int32_t)a.probe_col) : -1;
+    d.nref = a.nref;
+    for (uint32_t i = 0; i < a.nref; ++i) d.ref[i] = carry(a.ref[i]);
+    if (d.nslots == 0) d.slot_src[d.nslots++] = 0;  // keep one carried column for the ring
+    d.smem_groups = a.term == kTermGroupby ? a.smem_groups : 0;
+    const size_t smem = (size_t)kChainWarps * d.nslots * kRing * sizeof(int32_t) + (size_t)d.smem_groups * 16;
+    switch (a.term) {
+        case kTermAgg: return launch_chain_term<kTermAgg>(a, d, smem, s, ctx);
+        case kTermGroupby: return launch_chain_term<kTermGroupby>(a, d, smem, s, ctx);
+        default: return launch_chain_term<kTermSink>(a, d, smem, s, ctx);
+    }
+}
+
+}  // namespace mgv

@@ -16,6 +16,12 @@
 
 namespace mgv {
 
+// Home bucket of a key (radix-aware; see TableView).
+__device__ __forceinline__ uint32_t home_bucket(int32_t key, const TableView& t) {
+    const uint32_t part = ((uint32_t)key >> t.radix_shift) & t.radix_mask;
+    return part * t.bpp + __umulhi(murmur32((uint32_t)key), t.bpp);
+}
+
 __device__ __forceinline__ void table_insert(const TableView& t, int32_t key, int32_t pay,
                                              uint32_t* err, bool& dup, bool& ok) {
     ok = false;
@@ -27,7 +33,7 @@ __device__ __forceinline__ void table_insert(const TableView& t, int32_t key, in
         return;
     }
     const unsigned long long v = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
-    uint32_t b = bucket_of(key, t.nbuckets);
+    uint32_t b = home_bucket(key, t);
     for (uint32_t it = 0; it < t.nbuckets; ++it) {
         unsigned long long s[4];
         ld_bucket_relaxed(t.slots + 4ull * b, s);

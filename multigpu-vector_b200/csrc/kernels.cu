@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(kBlock, 2)
     while (tile < ntiles) {
         uint32_t w[R][8];
 #pragma unroll
-        for (int r = 0; r < R; ++r) ld_bucket(t.slots + 4ull * bucket_of(k[r], t.nbuckets), w[r]);
+        for (int r = 0; r < R; ++r) ld_bucket(t.slots + 4ull * home_bucket(k[r], t), w[r]);
 
         // Prefetch the next tile while the bucket loads are in flight.
         const uint64_t next = tile + gridDim.x;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kBlock, 2)
                 bool more;
                 match_bucket<UNIQUE>(w[r], k[r], mc, ms, more);
                 if (more) {
-                    const Matches x = probe_rest<UNIQUE>(t.slots, t.nbuckets, k[r], bucket_of(k[r], t.nbuckets));
+                    const Matches x = probe_rest<UNIQUE>(t.slots, t.nbuckets, k[r], home_bucket(k[r], t));
                     mc += x.count;
                     ms += (long long)x.sum;
                 }
@@ -297,249 +297,6 @@ cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t 
     }
     ctx->launches++;
     return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Generic chain: [select] -> [probe] -> sink
-//
-// Warp-ballot select as in unstable_select::consume_warp
-// (src/operators/select3.cu:19-85): each warp takes 128-row windows,
-// evaluates the predicate, and compacts the qualifying rows with
-// __ballot_sync/__popc into a per-warp shared-memory ring of 256 rows per
-// carried column, then pushes full 128-row vectors on (the reference's
-// 160-slot ring and consume_warp(x, 128)).  The downstream stage (probe,
-// sink) therefore always works on dense vectors.
-// ---------------------------------------------------------------------------
-
-struct ChainDev {
-    const int32_t* cols[MGV_MAX_COLS];
-    uint32_t ncols;
-    uint32_t sel_col;
-    int32_t sel_bound;
-    uint32_t probe_col;
-    uint64_t n;
-    TableView table;
-};
-
-__device__ __forceinline__ uint32_t pool_pop(PoolDev* p, uint32_t tries) {
-    for (uint32_t i = 0; i < tries; ++i) {
-        unsigned long long h = atomicAdd(&p->head, 0ull);
-        uint32_t top = (uint32_t)h;
-        if (top == kNil) return kNil;
-        uint32_t nxt = *((volatile uint32_t*)&p->next[top]);
-        unsigned long long nh = (((h >> 32) + 1ull) << 32) | nxt;
-        if (atomicCAS(&p->head, h, nh) == h) {
-            atomicSub(&p->available, 1u);
-            return top;
-        }
-    }
-    return kNil;
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Buffer id for chunk c of a sink; the warp that owns row c*capacity takes
-// a buffer from the pool and publishes it, everyone else waits for it with
-// a bounded wait (swap-on-full, src/buffer_manager.cuh:147-176).
-__device__ uint32_t sink_chunk(const SinkView& s, uint32_t c, bool opener, uint32_t* err) {
-    if (opener) {
-        uint32_t id = pool_pop(s.pool, 4096);
-        if (id == kNil) {
-            set_error(err, kDevOverflow, 3);
-            id = kNil - 1;  // published "no buffer" marker
-        }
-        atomicExch(s.chain + c, id);
-        return id;
-    }
-    const unsigned long long t0 = global_ns();
-    for (;;) {
-        uint32_t id = *((volatile uint32_t*)(s.chain + c));
-        if (id != kNil) return id;
-        if (global_ns() - t0 > 2000000000ull) {  // 2 s
-            set_error(err, kDevTimeout, 4);
-            return kNil - 1;
-        }
-        __nanosleep(64);
-    }
-}
-
-// Write `cnt` rows per lane, reserved warp-wide; vals(lane_row_index, col).
-template <class RowFn>
-__device__ __forceinline__ void sink_emit_warp(const SinkView& s, uint32_t my_cnt, RowFn row_val,
-                                               uint32_t* err) {
-    const uint32_t lane = lane_id();
-    uint32_t incl = my_cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    if (total == 0) return;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(s.cursor, (unsigned long long)total);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const unsigned long long limit = (unsigned long long)s.max_chunks * s.capacity;
-    // chunks touched by [base, base + total)
-    const unsigned long long first_c = base / s.capacity;
-    const unsigned long long last_c = (base + total - 1) / s.capacity;
-    // resolve chunk ids (lane j handles chunk first_c + j; at most 32 per call)
-    uint32_t my_chunk_id = kNil - 1;
-    const unsigned long long c = first_c + lane;
-    if (c <= last_c && c < s.max_chunks) {
-        const bool opener = c * s.capacity >= base;  // this warp owns the chunk's first row
-        my_chunk_id = sink_chunk(s, (uint32_t)c, opener, err);
-    }
-    if (lane == 0 && (last_c - first_c >= 32 || base + total > limit)) set_error(err, kDevOverflow, 5);
-    // Every lane runs the same number of iterations so that the chunk-id
-    // shuffle always reads from a converged lane.
-    const uint32_t maxc = __reduce_max_sync(0xffffffffu, my_cnt);
-    const unsigned long long pos0 = base + incl - my_cnt;
-    for (uint32_t i = 0; i < maxc; ++i) {
-        const bool act = i < my_cnt;
-        const unsigned long long pos = pos0 + i;
-        const unsigned long long rel = act ? pos / s.capacity - first_c : 0ull;
-        const uint32_t id = __shfl_sync(0xffffffffu, my_chunk_id, (int)(rel & 31ull));
-        if (!act || pos >= limit || rel >= 32 || id >= s.pool->nbuffers) continue;
-        const uint32_t off = (uint32_t)(pos % s.capacity);
-        int32_t* base_ptr = s.slab + (size_t)id * s.pool_ncols * s.capacity;
-        for (uint32_t col = 0; col < s.ncols; ++col)
-            base_ptr[(size_t)col * s.capacity + off] = row_val(i, col);
-    }
-}
-
-template <bool SEL, bool PROBE, bool UNIQUE>
-__global__ void __launch_bounds__(kBlock) k_chain_sink(ChainDev a, SinkView s, uint32_t* err) {
-    // per-warp ring: [ncols][256]
-    extern __shared__ int32_t smem[];
-    const uint32_t warp = threadIdx.x / kWarp, lane = lane_id();
-    int32_t* ring = smem + (size_t)warp * a.ncols * 256;
-    uint32_t head = 0, fill = 0;
-    const uint64_t nwin = (a.n + 127) / 128;
-    const uint64_t gwarp = (uint64_t)blockIdx.x * (kBlock / kWarp) + warp;
-    const uint64_t nwarps = (uint64_t)gridDim.x * (kBlock / kWarp);
-
-    // Process `cnt` (<= 128) dense rows starting at ring position `start`.
-    auto push_vector = [&](uint32_t start, uint32_t cnt) {
-        __syncwarp();
-#pragma unroll 1
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t idx = j * 32 + lane;
-            const bool in = idx < cnt;
-            const uint32_t rp = (start + idx) & 255u;
-            if (!PROBE) {
-                sink_emit_warp(s, in ? 1u : 0u,
-                               [&](uint32_t, uint32_t col) { return ring[col * 256 + rp]; }, err);
-            } else {
-                const int32_t key = in ? ring[a.probe_col * 256 + rp] : 0;
-                // pass 1: count matches
-                uint32_t m = 0;
-                if (in) {
-                    if (key == kEmptyKey) {
-                        m = (uint32_t)a.table.meta[0];
-                    } else {
-                        uint32_t b = bucket_of(key, a.table.nbuckets);
-                        for (uint32_t it = 0; it < a.table.nbuckets; ++it) {
-                            uint32_t w[8];
-                            ld_bucket(a.table.slots + 4ull * b, w);
-                            uint32_t c;
-                            long long sdum;
-                            bool more;
-                            match_bucket<UNIQUE>(w, key, c, sdum, more);
-                            m += c;
-                            if (!more) break;
-                            b = (b + 1 == a.table.nbuckets) ? 0u : b + 1;
-                        }
-                    }
-                }
-                // pass 2: emit the i-th match's payload
-                const uint32_t side_n = (uint32_t)min((unsigned long long)a.table.meta[0],
-                                                      (unsigned long long)a.table.side_cap);
-                sink_emit_warp(
-                    s, m,
-                    [&](uint32_t i, uint32_t col) -> int32_t {
-                        if (col < a.ncols) return ring[col * 256 + rp];
-                        // build payload of the i-th match
-                        if (key == kEmptyKey) return i < side_n ? a.table.side_pay[i] : 0;
-                        uint32_t b = bucket_of(key, a.table.nbuckets);
-                        uint32_t seen = 0;
-                        for (uint32_t it = 0; it < a.table.nbuckets; ++it) {
-                            uint32_t w[8];
-                            ld_bucket(a.table.slots + 4ull * b, w);
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                if (w[2 * q] == (uint32_t)key) {
-                                    if (seen == i) return (int32_t)w[2 * q + 1];
-                                    ++seen;
-                                }
-                            }
-                            if (w[6] == (uint32_t)kEmptyKey) break;
-                            b = (b + 1 == a.table.nbuckets) ? 0u : b + 1;
-                        }
-                        return 0;
-                    },
-                    err);
-            }
-        }
-        __syncwarp();
-    };
-
-    for (uint64_t win = gwarp; win < nwin; win += nwarps) {
-        const uint64_t r0 = win * 128;
-#pragma unroll 1
-        for (int j = 0; j < 4; ++j) {
-            const uint64_t row = r0 + j * 32 + lane;
-            bool pass = row < a.n;
-            if (SEL && pass) pass = a.cols[a.sel_col][row] <= a.sel_bound;
-            const unsigned m = __ballot_sync(0xffffffffu, pass);
-            if (pass) {
-                const uint32_t pos = (head + fill + __popc(m & ((1u << lane) - 1u))) & 255u;
-                for (uint32_t c = 0; c < a.ncols; ++c) ring[c * 256 + pos] = a.cols[c][row];
-            }
-            fill += __popc(m);
-            if (fill >= 128) {
-                push_vector(head, 128);
-                head = (head + 128) & 255u;
-                fill -= 128;
-            }
-        }
-    }
-    if (fill) push_vector(head, fill);
-}
-
-cudaError_t launch_chain_sink(const ChainArgs& a, const SinkView& sink, cudaStream_t s,
-                              Context* ctx) {
-    if (a.n == 0) return cudaSuccess;
-    ChainDev d{};
-    for (uint32_t c = 0; c < a.ncols; ++c) d.cols[c] = a.cols[c];
-    d.ncols = a.ncols;
-    d.sel_col = a.sel_col;
-    d.sel_bound = a.sel_bound;
-    d.probe_col = a.probe_col;
-    d.n = a.n;
-    d.table = a.table;
-    const size_t smem = (size_t)(kBlock / kWarp) * a.ncols * 256 * sizeof(int32_t);
-    const void* k;
-    if (a.has_probe)
-        k = a.has_sel ? (a.unique ? (const void*)k_chain_sink<true, true, true> : (const void*)k_chain_sink<true, true, false>)
-                      : (a.unique ? (const void*)k_chain_sink<false, true, true> : (const void*)k_chain_sink<false, true, false>);
-    else
-        k = a.has_sel ? (const void*)k_chain_sink<true, false, false> : (const void*)k_chain_sink<false, false, false>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    int grid = occupancy_grid(k, kBlock, smem, ctx);
-    const uint64_t need = ((a.n + 127) / 128 + kBlock / kWarp - 1) / (kBlock / kWarp);
-    if ((uint64_t)grid > need) grid = (int)need;
-    void* args[] = {(void*)&d, (void*)&sink, (void*)&ctx->d_err};
-    cudaError_t e = cudaLaunchKernel(k, dim3(grid), dim3(kBlock), args, smem, s);
-    ctx->launches++;
-    return e;
 }
 
 }  // namespace mgv

@@ -33,13 +33,30 @@ mgv_status cuda_fail(cudaError_t e, const char* what);
 struct TableView {
     unsigned long long* slots;
     uint32_t nbuckets;
-    uint32_t pad;
+    // Radix layout: the home bucket of a key lies in the region of its
+    // partition ((key >> radix_shift) & radix_mask), bpp buckets per region;
+    // radix_mask 0 and bpp == nbuckets for an unpartitioned table.  Runs
+    // continue linearly across regions.
+    uint32_t radix_shift;
+    uint32_t radix_mask;
+    uint32_t bpp;
     // Rows whose key is the reserved empty marker INT32_MIN:
     // meta[0] = their count, meta[1] = their payload sum, meta[2] = rows
     // inserted into the table, meta[3] = duplicate-key flag.
     unsigned long long* meta;
     int32_t* side_pay;      // payloads of those rows (for emitting matches)
     uint64_t side_cap;
+};
+
+// Group-by table in global memory: cap (power of two) slots of {key, sum,
+// count}, empty key INT32_MIN; the group INT32_MIN has its own counters.
+struct GroupTableView {
+    int32_t* keys;
+    unsigned long long* sums;
+    unsigned long long* counts;
+    unsigned long long* special;  // [0] sum, [1] count of group INT32_MIN
+    uint32_t cap;
+    uint32_t pad;
 };
 
 // Output rows appended to a chain of pool buffers.
@@ -93,11 +110,11 @@ struct Context {
     // pinned landing zone for close(): [0..1] error word, [2..] result words
     unsigned long long* h_stage = nullptr;
     std::atomic<uint64_t> launches{0};
-    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, {0u, 0u, 0u}};
+    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, 4096u, {0u, 0u}};
     std::mutex mu;
 };
 
-enum class OpKind { Select, Aggregate, HashBuild, HashProbe, Sink };
+enum class OpKind { Select, Aggregate, HashBuild, HashProbe, Sink, Groupby, Partition };
 enum class OpState { Created, Open, Closed };
 
 struct Op {
@@ -126,6 +143,18 @@ struct Op {
     SinkView sink{};
     uint64_t sink_rows = 0;
     std::vector<uint32_t> sink_chain;
+    // group-by
+    mgv_groupby_desc gb{};
+    GroupTableView gtab{};
+    std::vector<mgv_group_row> gb_rows;
+    // partition
+    mgv_partition_desc pt{};
+    int32_t* pt_store = nullptr;          // ncols x capacity, partition-major runs
+    uint32_t pt_ncols = 0;
+    uint64_t pt_fill = 0;                 // rows stored
+    unsigned long long* pt_dev = nullptr; // [P] histogram / cursors
+    std::vector<uint64_t> pt_hist;        // rows per partition (all runs)
+    std::vector<std::pair<uint64_t, uint64_t>> pt_runs;  // (first row, rows)
     // device allocations owned by this op
     std::vector<void*> allocs;
 };
@@ -154,7 +183,9 @@ cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, ui
 cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t n,
                              const TableView& t, bool unique, uint32_t sum_mode,
                              unsigned long long* acc, cudaStream_t s, Context* ctx);
-// Generic fused chain: [select] -> [probe] -> sink.
+// Generic fused chain (chain.cu): [select] -> [probe] -> terminal.
+enum TermKind : int { kTermAgg = 0, kTermGroupby = 1, kTermSink = 2 };
+
 struct ChainArgs {
     const int32_t* cols[MGV_MAX_COLS];
     uint32_t ncols;
@@ -166,9 +197,28 @@ struct ChainArgs {
     uint32_t probe_col;
     TableView table;
     bool unique;
+    int term;
+    // terminal column references (input column, ncols = build payload, -1 none):
+    //   aggregate: ref[0], ref[1] summed;  group-by: ref[0] group, ref[1] value;
+    //   sink: ref[i] = source of output column i
+    int32_t ref[MGV_MAX_COLS + 2];
+    uint32_t nref;
+    unsigned long long* acc;
+    GroupTableView gt;
+    uint32_t smem_groups;
+    SinkView sink;
 };
-cudaError_t launch_chain_sink(const ChainArgs& a, const SinkView& sink, cudaStream_t s,
-                              Context* ctx);
+cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx);
+
+// partition.cu
+cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,
+                                  int32_t sel_bound, uint32_t key_col, uint32_t shift, uint32_t bits,
+                                  unsigned long long* hist, cudaStream_t s, Context* ctx);
+cudaError_t launch_partition_scatter(const int32_t* const* cols, uint32_t ncols, uint64_t n, bool has_sel,
+                                     uint32_t sel_col, int32_t sel_bound, uint32_t key_col, uint32_t shift,
+                                     uint32_t bits, unsigned long long* cursors, int32_t* out, uint64_t out_stride,
+                                     cudaStream_t s, Context* ctx);
+cudaError_t launch_fill_i32(int32_t* p, uint64_t n, int32_t v, cudaStream_t s, Context* ctx);
 
 // pool.cu
 cudaError_t pool_init_device(Pool* p);

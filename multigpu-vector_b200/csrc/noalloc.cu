@@ -99,6 +99,9 @@ extern "C" mgv_status mgv_hash_join_noalloc(int device, const int32_t* build_key
     TableView t{};
     t.slots = reinterpret_cast<unsigned long long*>(slot->scratch);
     t.nbuckets = kBuckets;
+    t.bpp = kBuckets;
+    t.radix_mask = 0;
+    t.radix_shift = 0;
     t.side_pay = reinterpret_cast<int32_t*>(slot->scratch + kTableBytes);
     t.side_cap = kMaxBuildRows;
     t.meta = reinterpret_cast<unsigned long long*>(slot->scratch + kTableBytes + kSideBytes);

@@ -1,0 +1,147 @@
+// partition.cu -- the exchange reduced to an in-GPU radix partitioner.
+//
+// The reference's split (src/operators/split.cu:49-118) routes each row to
+// one of its parents by hash3(x) = x & 1, ballot-compacting per destination
+// into 160-row staging areas in global memory.  Here a [select] -> partition
+// consume makes two passes over its input:
+//   1. k_part_hist: per-CTA shared histograms of (key >> shift) & mask,
+//      merged with one global atomic per partition and CTA;
+//   2. k_part_scatter: tiles of 1024 rows get a local rank per row from a
+//      shared-memory histogram, reserve one contiguous range per partition
+//      from the global cursors (host-initialised to the exclusive prefix sum),
+//      and write every column of the row to its place.
+// The result is partition-major storage that close() replays into the
+// parent chain, so a radix-laid-out hash table is built one region at a time.
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "mgv_internal.h"
+
+namespace mgv {
+namespace {
+
+constexpr int kPartBlock = 256;
+constexpr int kPartRows = 4;  // rows per thread per tile
+
+template <bool SEL>
+__global__ void __launch_bounds__(kPartBlock)
+    k_part_hist(const int32_t* __restrict__ keys, const int32_t* __restrict__ filt, int32_t bound, uint64_t n,
+                uint32_t shift, uint32_t mask, unsigned long long* hist) {
+    extern __shared__ uint32_t sh[];
+    for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock) sh[p] = 0;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * kPartBlock + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kPartBlock) {
+        if (SEL && !(__ldg(filt + i) <= bound)) continue;
+        atomicAdd(&sh[((uint32_t)__ldg(keys + i) >> shift) & mask], 1u);
+    }
+    __syncthreads();
+    for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock)
+        if (sh[p]) atomicAdd(hist + p, (unsigned long long)sh[p]);
+}
+
+struct ScatterCols {
+    const int32_t* cols[MGV_MAX_COLS];
+};
+
+template <bool SEL>
+__global__ void __launch_bounds__(kPartBlock)
+    k_part_scatter(ScatterCols in, uint32_t ncols, uint32_t key_col, const int32_t* __restrict__ filt, int32_t bound,
+                   uint64_t n, uint32_t shift, uint32_t mask, unsigned long long* cursors, int32_t* out,
+                   uint64_t out_stride) {
+    extern __shared__ unsigned long long shb[];  // [P] reserved bases, then [P] u32 counts
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(shb + (mask + 1));
+    constexpr uint64_t kTile = (uint64_t)kPartBlock * kPartRows;
+    const uint64_t ntiles = (n + kTile - 1) / kTile;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock) cnt[p] = 0;
+        __syncthreads();
+        uint32_t part[kPartRows], rank[kPartRows];
+        bool keep[kPartRows];
+#pragma unroll
+        for (int r = 0; r < kPartRows; ++r) {
+            const uint64_t i = tile * kTile + (uint64_t)r * kPartBlock + threadIdx.x;
+            keep[r] = i < n;
+            if (SEL && keep[r]) keep[r] = __ldg(filt + i) <= bound;
+            part[r] = keep[r] ? (((uint32_t)__ldg(in.cols[key_col] + i) >> shift) & mask) : 0u;
+            rank[r] = keep[r] ? atomicAdd(&cnt[part[r]], 1u) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock)
+            shb[p] = cnt[p] ? atomicAdd(cursors + p, (unsigned long long)cnt[p]) : 0ull;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kPartRows; ++r) {
+            if (!keep[r]) continue;
+            const uint64_t i = tile * kTile + (uint64_t)r * kPartBlock + threadIdx.x;
+            const uint64_t dst = shb[part[r]] + rank[r];
+            for (uint32_t c = 0; c < ncols; ++c) out[(uint64_t)c * out_stride + dst] = __ldg(in.cols[c] + i);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,
+                                  int32_t sel_bound, uint32_t key_col, uint32_t shift, uint32_t bits,
+                                  unsigned long long* hist, cudaStream_t s, Context* ctx) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t mask = (1u << bits) - 1u;
+    const size_t smem = sizeof(uint32_t) * (mask + 1);
+    const void* k = has_sel ? (const void*)k_part_hist<true> : (const void*)k_part_hist<false>;
+    int grid = occupancy_grid(k, kPartBlock, smem, ctx);
+    const uint64_t need = (n + kPartBlock - 1) / kPartBlock;
+    if ((uint64_t)grid > need) grid = (int)need;
+    if (has_sel)
+        k_part_hist<true><<<grid, kPartBlock, smem, s>>>(cols[key_col], cols[sel_col], sel_bound, n, shift, mask, hist);
+    else
+        k_part_hist<false><<<grid, kPartBlock, smem, s>>>(cols[key_col], nullptr, 0, n, shift, mask, hist);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_partition_scatter(const int32_t* const* cols, uint32_t ncols, uint64_t n, bool has_sel,
+                                     uint32_t sel_col, int32_t sel_bound, uint32_t key_col, uint32_t shift,
+                                     uint32_t bits, unsigned long long* cursors, int32_t* out, uint64_t out_stride,
+                                     cudaStream_t s, Context* ctx) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t mask = (1u << bits) - 1u;
+    ScatterCols in{};
+    for (uint32_t c = 0; c < ncols; ++c) in.cols[c] = cols[c];
+    const size_t smem = (sizeof(unsigned long long) + sizeof(uint32_t)) * (mask + 1);
+    const void* k = has_sel ? (const void*)k_part_scatter<true> : (const void*)k_part_scatter<false>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int grid = occupancy_grid(k, kPartBlock, smem, ctx);
+    const uint64_t need = (n + kPartBlock * kPartRows - 1) / (kPartBlock * kPartRows);
+    if ((uint64_t)grid > need) grid = (int)need;
+    const int32_t* filt = has_sel ? cols[sel_col] : nullptr;
+    if (has_sel)
+        k_part_scatter<true><<<grid, kPartBlock, smem, s>>>(in, ncols, key_col, filt, sel_bound, n, shift, mask,
+                                                            cursors, out, out_stride);
+    else
+        k_part_scatter<false><<<grid, kPartBlock, smem, s>>>(in, ncols, key_col, filt, sel_bound, n, shift, mask,
+                                                             cursors, out, out_stride);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+// ---- int32 fill (group table keys) ------------------------------------------
+
+__global__ void k_fill_i32(int32_t* p, uint64_t n, int32_t v) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+cudaError_t launch_fill_i32(int32_t* p, uint64_t n, int32_t v, cudaStream_t s, Context* ctx) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->prop.multiProcessorCount * 8;
+    k_fill_i32<<<(int)(want < cap ? want : cap), 256, 0, s>>>(p, n, v);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+}  // namespace mgv

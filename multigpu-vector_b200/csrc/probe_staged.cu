@@ -134,7 +134,7 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
     uint32_t w[R][8];
 #pragma unroll
     for (int r = 0; r < R; ++r)
-        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * bucket_of(rk[32 * r], t.nbuckets), w[r]);
+        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * home_bucket(rk[32 * r], t), w[r]);
     uint32_t wc[8];
     if (has_c) ld_bucket(t.slots + 4ull * cb, wc);
     __syncwarp();  // every lane has read its queue entry before anyone appends
@@ -149,7 +149,7 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
         if (key == kEmptyKey) {
             fold_reserved<ADD_BP, ADD_PP>(t, pay, a);
         } else if (fold<UNIQUE, ADD_BP, ADD_PP>(w[r], key, pay, a)) {
-            enqueue<Q>(q, key, pay, next_bucket(bucket_of(key, t.nbuckets), t.nbuckets));
+            enqueue<Q>(q, key, pay, next_bucket(home_bucket(key, t), t.nbuckets));
         }
     }
     if (has_c && fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a)) enqueue<Q>(q, ck, cp, next_bucket(cb, t.nbuckets));

@@ -51,7 +51,8 @@ class CtxInfo(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("probe_kernel", c_uint32), ("probe_rows_per_thread", c_uint32), ("probe_stages", c_uint32),
-                ("probe_ctas_per_sm", c_uint32), ("default_load_factor", c_float), ("reserved", c_uint32 * 3)]
+                ("probe_ctas_per_sm", c_uint32), ("default_load_factor", c_float),
+                ("groupby_smem_slots", c_uint32), ("reserved", c_uint32 * 2)]
 
 
 class PoolStats(ctypes.Structure):
@@ -74,7 +75,8 @@ class AggResult(ctypes.Structure):
 
 class HashBuildDesc(ctypes.Structure):
     _fields_ = [("key_col", c_uint32), ("payload_col", c_int32), ("expected_rows", c_uint64),
-                ("load_factor", c_float), ("reserved", c_uint32)]
+                ("load_factor", c_float), ("radix_bits", c_uint32), ("radix_shift", c_uint32),
+                ("reserved", c_uint32)]
 
 
 class HashBuildInfo(ctypes.Structure):
@@ -84,6 +86,19 @@ class HashBuildInfo(ctypes.Structure):
 
 class HashProbeDesc(ctypes.Structure):
     _fields_ = [("key_col", c_uint32), ("reserved", c_uint32), ("build", c_void_p)]
+
+
+class GroupbyDesc(ctypes.Structure):
+    _fields_ = [("group_col", c_uint32), ("value_col", c_int32), ("max_groups", c_uint32), ("reserved", c_uint32)]
+
+
+class GroupRow(ctypes.Structure):
+    _fields_ = [("group", c_int32), ("pad", c_int32), ("sum", c_int64), ("count", c_int64)]
+
+
+class PartitionDesc(ctypes.Structure):
+    _fields_ = [("key_col", c_uint32), ("radix_bits", c_uint32), ("radix_shift", c_uint32), ("reserved", c_uint32),
+                ("max_rows", c_uint64)]
 
 
 class SinkDesc(ctypes.Structure):
@@ -133,6 +148,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_op_create_hash_build": (st, [c_void_p, POINTER(HashBuildDesc), POINTER(c_void_p)]),
         "mgv_op_create_hash_probe": (st, [c_void_p, POINTER(HashProbeDesc), c_void_p, POINTER(c_void_p)]),
         "mgv_op_create_sink": (st, [c_void_p, POINTER(SinkDesc), POINTER(c_void_p)]),
+        "mgv_op_create_groupby": (st, [c_void_p, POINTER(GroupbyDesc), POINTER(c_void_p)]),
+        "mgv_op_create_partition": (st, [c_void_p, POINTER(PartitionDesc), c_void_p, POINTER(c_void_p)]),
         "mgv_op_destroy": (st, [c_void_p]),
         "mgv_op_open": (st, [c_void_p, c_void_p]),
         "mgv_op_consume": (st, [c_void_p, POINTER(Buffer), c_void_p]),
@@ -313,9 +330,10 @@ class Op:
         return cls(ctx, h, "aggregate")
 
     @classmethod
-    def hash_build(cls, ctx, key_col: int, payload_col: int, expected_rows: int, load_factor: float = 0.0) -> "Op":
+    def hash_build(cls, ctx, key_col: int, payload_col: int, expected_rows: int, load_factor: float = 0.0,
+                   radix_bits: int = 0, radix_shift: int = 0) -> "Op":
         h = c_void_p()
-        d = HashBuildDesc(key_col, payload_col, expected_rows, load_factor, 0)
+        d = HashBuildDesc(key_col, payload_col, expected_rows, load_factor, radix_bits, radix_shift, 0)
         _call("mgv_op_create_hash_build", ctx.h, byref(d), byref(h))
         return cls(ctx, h, "hash_build")
 
@@ -325,6 +343,21 @@ class Op:
         _call("mgv_op_create_hash_probe", ctx.h, byref(HashProbeDesc(key_col, 0, build.h.value)), parent.h, byref(h))
         op = cls(ctx, h, "hash_probe", parent)
         op.build = build
+        return op
+
+    @classmethod
+    def groupby(cls, ctx, group_col: int, value_col: int, max_groups: int) -> "Op":
+        h = c_void_p()
+        _call("mgv_op_create_groupby", ctx.h, byref(GroupbyDesc(group_col, value_col, max_groups, 0)), byref(h))
+        return cls(ctx, h, "groupby")
+
+    @classmethod
+    def partition(cls, ctx, key_col: int, radix_bits: int, radix_shift: int, max_rows: int, parent: "Op") -> "Op":
+        h = c_void_p()
+        d = PartitionDesc(key_col, radix_bits, radix_shift, 0, max_rows)
+        _call("mgv_op_create_partition", ctx.h, byref(d), parent.h, byref(h))
+        op = cls(ctx, h, "partition", parent)
+        op.radix_bits = radix_bits
         return op
 
     @classmethod
@@ -365,6 +398,17 @@ class Op:
             r = c_uint64()
             _call("mgv_op_result", self.h, byref(r), ctypes.sizeof(r), None)
             return r.value
+        if self.kind == "groupby":
+            need = c_size_t()
+            _call("mgv_op_result", self.h, None, 0, byref(need))
+            n = need.value // ctypes.sizeof(GroupRow)
+            arr = (GroupRow * max(1, n))()
+            _call("mgv_op_result", self.h, arr, ctypes.sizeof(arr), None)
+            return [(r.group, r.sum, r.count) for r in arr[:n]]
+        if self.kind == "partition":
+            arr = (c_uint64 * (1 << self.radix_bits))()
+            _call("mgv_op_result", self.h, arr, ctypes.sizeof(arr), None)
+            return list(arr)
         raise MgvError(EINVAL, "result", f"{self.kind} has no result")
 
     def sink_read(self, col: int, dst_ptr: int, max_rows: int) -> int:
@@ -400,6 +444,24 @@ def create_sum_select_pipeline(ctx: Context, bound: int, filter_col: int = 0, su
     agg = Op.aggregate(ctx, sum_col, -1)
     sel = Op.select(ctx, filter_col, bound, agg)
     return sel, agg
+
+
+def create_join_groupby_pipeline(ctx: Context, build_rows: int, probe_max_groups: int, filter_bound: int,
+                                 radix_bits: int = 8, load_factor: float = 0.0):
+    """select -> hash join -> group-by with a radix-partitioned build.
+
+    Build side columns: (key,); partitioned on `radix_bits` key bits (the
+    reference's split / hash_exchange, src/main9.cu:104-148, reduced to one
+    GPU) into a radix-laid-out table.  Probe side columns: (key, filter,
+    group, value): select(filter <= filter_bound) -> hash_probe(key) ->
+    group-by(group): int64 SUM(value), COUNT.  Returns
+    (build_head, build, probe_head, groupby)."""
+    hb = Op.hash_build(ctx, 0, -1, build_rows, load_factor, radix_bits, 0)
+    part = Op.partition(ctx, 0, radix_bits, 0, max(build_rows, 1), hb) if radix_bits else hb
+    gb = Op.groupby(ctx, 2, 3, probe_max_groups)
+    probe = Op.hash_probe(ctx, 0, hb, gb)
+    sel = Op.select(ctx, 1, filter_bound, probe)
+    return part, hb, sel, gb
 
 
 def create_count_join_1G_pipeline(ctx: Context, build_rows: int, load_factor: float = 0.0,

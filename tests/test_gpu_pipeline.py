@@ -1,0 +1,152 @@
+"""select -> hash join -> group-by, the radix partitioner, and the generic
+fused chain, on the GPU against the oracle.
+
+The pipeline is the reference's count_join_select plan shape
+(src/main9.cu:260-324: split/hash_exchange before the build, select before
+the probe) with the exchange reduced to an in-GPU 8-bit radix partition and
+the count widened to a per-group int64 SUM/COUNT."""
+import os
+
+import numpy as np
+import pytest
+
+import mgv
+import pyoracle as po
+from gpu_util import dev, sorted_rows
+
+pytestmark = pytest.mark.gpu
+
+
+def config3_inputs(nb, npb, groups=4096, seed=0x5EED0901, key_range=None):
+    bk = po.gen_perm(nb, seed)
+    pkey = po.gen_uniform(npb, seed, 1, 0, key_range or nb)
+    pfil = po.gen_uniform(npb, seed, 2, 0, 1000)
+    pgrp = po.gen_zipf(npb, seed, 3, groups)
+    pval = po.gen_uniform(npb, seed, 4, 0, 1 << 16)
+    return bk, pkey, pfil, pgrp, pval
+
+
+def run_pipeline(ctx, torch, bk, probe_cols, groups, bound, radix_bits=8):
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, bk.size, groups, bound, radix_bits)
+    part.open(); part.consume_columns([dev(torch, bk)], bk.size); part.close()
+    info = hb.result()
+    sel.open(); sel.consume_columns([dev(torch, c) for c in probe_cols], probe_cols[0].size); sel.close()
+    r = gb.result()
+    for o in (sel, gb, hb, part):
+        o.destroy()
+    return r, info
+
+
+@pytest.mark.parametrize("radix_bits", [0, 4, 8])
+@pytest.mark.parametrize("nb,npb", [(1 << 12, 1 << 16), (1 << 16, 1 << 20), (100003, 3000017)])
+def test_select_join_groupby(ctx, torch_cuda, radix_bits, nb, npb):
+    bk, pkey, pfil, pgrp, pval = config3_inputs(nb, npb, key_range=nb + nb // 8)  # some keys miss
+    got, info = run_pipeline(ctx, torch_cuda, bk, [pkey, pfil, pgrp, pval], 4096, 99, radix_bits)
+    want, _, _ = po.run_query(bk, pkey, pfil, pgrp, pval, 99)
+    assert got == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want]
+    assert info.rows == nb
+
+
+def test_config3_full_size(ctx, torch_cuda):
+    """probe 2^27 rows, build 2^24 keys, 10% selectivity, Zipf(1) over 4096 groups."""
+    torch = torch_cuda
+    nb, npb = 1 << 24, 1 << 27
+    cols = [torch.empty(npb, dtype=torch.int32, device="cuda") for _ in range(4)]
+    bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+    seed = 0x5EED0003
+    ctx.gen_perm(bk, nb, seed)
+    ctx.gen_uniform(cols[0], npb, seed, 1, 0, nb)
+    ctx.gen_uniform(cols[1], npb, seed, 2, 0, 1000)
+    ctx.gen_zipf(cols[2], npb, seed, 3, 4096)
+    ctx.gen_uniform(cols[3], npb, seed, 4, 0, 1 << 16)
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8)
+    part.open(); part.consume_columns([bk], nb); part.close()
+    sel.open(); sel.consume_columns(cols, npb); sel.close()
+    got = gb.result()
+    host = [c.cpu().numpy() for c in cols]
+    want, tc, ts = po.run_query(bk.cpu().numpy(), *host, 99)
+    assert got == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want]
+    # every probe key is a build key: the count is the number of qualifying rows
+    assert sum(c for _, _, c in got) == int((host[1] <= 99).sum())
+    for o in (sel, gb, hb, part):
+        o.destroy()
+
+
+def test_partition_histogram_and_rows(ctx, torch_cuda):
+    torch = torch_cuda
+    n = 200003
+    k = po.gen_uniform(n, 0x5EED0902, 0, -(1 << 31), 1 << 32)
+    v = po.gen_uniform(n, 0x5EED0902, 1, 0, 1000)
+    pool = mgv.Pool(ctx, 16, 1 << 15, 2)
+    sink = mgv.Op.sink(ctx, pool)
+    part = mgv.Op.partition(ctx, 0, 8, 3, n, sink)
+    part.open()
+    part.consume_columns([dev(torch, k[:n // 2]), dev(torch, v[:n // 2])], n // 2)   # two runs
+    part.consume_columns([dev(torch, k[n // 2:]), dev(torch, v[n // 2:])], n - n // 2)
+    part.close()
+    hist = part.result()
+    want_hist, _, _ = po.partition(k, 8, 3)
+    assert hist == [int(x) for x in want_hist]
+    rows = sink.result()
+    assert rows == n
+    out = [torch.empty(rows, dtype=torch.int32, device="cuda") for _ in range(2)]
+    for c in range(2):
+        sink.sink_read(c, out[c].data_ptr(), rows)
+    got = sorted_rows([o.cpu().numpy() for o in out])
+    assert np.array_equal(got, sorted_rows([k, v]))
+    for o in (part, sink):
+        o.destroy()
+    pool.destroy()
+
+
+def test_select_partition_aggregate(ctx, torch_cuda):
+    n = 100000
+    f = po.gen_uniform(n, 0x5EED0903, 0, 0, 100)
+    k = po.gen_uniform(n, 0x5EED0903, 1, 0, 1 << 20)
+    agg = mgv.Op.aggregate(ctx, 1, -1)
+    part = mgv.Op.partition(ctx, 1, 4, 0, n, agg)
+    sel = mgv.Op.select(ctx, 0, 49, part)
+    sel.open(); sel.consume_columns([dev(torch_cuda, f), dev(torch_cuda, k)], n); sel.close()
+    assert agg.result() == po.select_agg(f, k, 49)
+    for o in (sel, part, agg):
+        o.destroy()
+
+
+@pytest.mark.parametrize("dup", [False, True])
+def test_select_probe_aggregate_and_sink(ctx, torch_cuda, dup):
+    """The generic chain with a select before the probe, both terminals."""
+    torch = torch_cuda
+    nb, npb = 5000, 200003
+    bk = po.gen_uniform(nb, 0x5EED0904, 0, 0, 2000) if dup else po.gen_perm(nb, 0x5EED0904)
+    bp = po.gen_uniform(nb, 0x5EED0904, 1, -(1 << 20), 1 << 21)
+    pk = po.gen_uniform(npb, 0x5EED0904, 2, 0, 6000)
+    pf = po.gen_uniform(npb, 0x5EED0904, 3, 0, 100)
+    pp = po.gen_uniform(npb, 0x5EED0904, 4, -(1 << 20), 1 << 21)
+    hb = mgv.Op.hash_build(ctx, 0, 1, nb)
+    hb.open(); hb.consume_columns([dev(torch, bk), dev(torch, bp)], nb); hb.close()
+    keep = pf <= 30
+    chain = po.Chain(bk, bp)
+    # aggregate: COUNT + SUM(bp + pp) over the selected probe rows
+    agg = mgv.Op.aggregate(ctx, 3, 2)        # build payload is column 3 (= ncols)
+    pr = mgv.Op.hash_probe(ctx, 0, hb, agg)
+    sel = mgv.Op.select(ctx, 1, 30, pr)
+    d = [dev(torch, pk), dev(torch, pf), dev(torch, pp)]
+    sel.open(); sel.consume_columns(d, npb); sel.close()
+    assert agg.result() == chain.probe_agg(pk[keep], pp[keep])
+    # sink: (key, filter, pp, bp) rows
+    pool = mgv.Pool(ctx, 64, 1 << 15, 4)
+    sink = mgv.Op.sink(ctx, pool)
+    pr2 = mgv.Op.hash_probe(ctx, 0, hb, sink)
+    sel2 = mgv.Op.select(ctx, 1, 30, pr2)
+    sel2.open(); sel2.consume_columns(d, npb); sel2.close()
+    rows = sink.result()
+    out = [torch.empty(max(rows, 1), dtype=torch.int32, device="cuda") for _ in range(4)]
+    for c in range(4):
+        sink.sink_read(c, out[c].data_ptr(), rows)
+    o = [x.cpu().numpy()[:rows] for x in out]
+    got = sorted_rows([o[0], o[3], o[2]])               # key, bp, pp
+    want = chain.probe_emit(pk[keep], pp[keep])
+    assert np.array_equal(got, want.astype(np.int64))
+    for x in (sel, pr, agg, sel2, pr2, sink, hb):
+        x.destroy()
+    pool.destroy()
