@@ -314,6 +314,116 @@ mgv_status mgv_gen_probe_keys(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t s
 mgv_status mgv_gen_zipf(mgv_ctx *ctx, int32_t *dst, uint64_t n, uint64_t seed, uint32_t stream_id,
                         uint32_t groups, double s, void *stream);
 
+/* ---- batched queries ---------------------------------------------------- */
+/*
+ * Many independent select -> hash join -> group-by queries executed
+ * together: per-query tables in one device arena, one persistent build
+ * launch and one persistent probe launch over (query, rows) work items,
+ * results packed into one copy to the host, the whole sequence captured
+ * once and replayed as a CUDA graph.  No reference counterpart (the
+ * reference runs one pipeline per plan, src/main9.cu:371-631).
+ */
+typedef struct mgv_query_desc {
+    const int32_t *build_keys;      /* device columns                          */
+    const int32_t *build_payloads;  /* may be NULL                             */
+    uint64_t build_rows;
+    const int32_t *probe_key;
+    const int32_t *probe_filter;
+    const int32_t *probe_group;
+    const int32_t *probe_value;
+    uint64_t probe_rows;
+    int32_t filter_bound;           /* rows with filter <= bound are probed    */
+    uint32_t max_groups;            /* upper bound on distinct groups          */
+} mgv_query_desc;
+
+typedef struct mgv_batch_config {
+    float load_factor;          /* join tables (0 = the context's default)      */
+    uint32_t build_item_rows;   /* rows per build work item (0 = 65536)         */
+    uint32_t probe_item_rows;   /* rows per probe work item (0 = 32768)         */
+    uint32_t probe_ctas_per_sm; /* 0 = as many as fit                           */
+    uint32_t use_graph;         /* 1 = capture once, replay as a CUDA graph     */
+    uint32_t reserved[3];
+} mgv_batch_config;
+
+typedef struct mgv_batch mgv_batch;
+
+typedef struct mgv_batch_stats {
+    uint64_t arena_bytes;
+    uint32_t queries, build_items, probe_items, graph;
+    double last_run_ms;         /* host wall clock of the last run (incl. the copy to host) */
+} mgv_batch_stats;
+
+/* config NULL: the configuration the context's autotuner chose last, else defaults. */
+mgv_status mgv_batch_create(mgv_ctx *ctx, const mgv_query_desc *queries, uint32_t nq,
+                            const mgv_batch_config *config, mgv_batch **out);
+/* Runs every query; results are on the host when it returns. */
+mgv_status mgv_batch_run(mgv_batch *b, void *stream);
+/* The same queries one at a time through the plain operator pipeline
+ * (partition-free select -> hash_probe -> groupby after a hash_build), the
+ * comparison baseline; its results are kept apart from the batch's. */
+mgv_status mgv_batch_run_plain(mgv_batch *b, void *stream);
+/* Groups of query q sorted by group (plain = 1: of the last plain run). */
+mgv_status mgv_batch_result(mgv_batch *b, uint32_t q, int plain, mgv_group_row *out, uint64_t cap,
+                            uint64_t *rows);
+mgv_status mgv_batch_stats_get(mgv_batch *b, mgv_batch_stats *out);
+mgv_status mgv_batch_destroy(mgv_batch *b);
+/* Project autotuner: times candidate configurations (load factor, probe
+ * item rows, CTAs per SM) on these queries and returns the fastest; the
+ * context remembers it for mgv_batch_create(config = NULL). */
+mgv_status mgv_batch_autotune(mgv_ctx *ctx, const mgv_query_desc *queries, uint32_t nq, mgv_batch_config *out);
+
+/* ---- serving ------------------------------------------------------------ */
+/*
+ * A query server with continuous batching over resident build tables (no
+ * reference counterpart).  Requests (select -> join -> group-by against a
+ * registered table) may be submitted at any time; a scheduler thread
+ * admits them in arrival order while `memory_budget` bytes of device memory
+ * allow (group table and result region per request, plus the resident
+ * tables), launches admitted requests together as one batch on a free
+ * stream, and keeps up to `max_inflight` batches on the GPU, so requests
+ * arriving while others run are admitted as streams and memory free up.
+ * plain = 1 serves requests one at a time through the operator API instead
+ * (the per-query baseline).
+ */
+typedef struct mgv_server_config {
+    uint64_t memory_budget;  /* bytes for resident tables + in-flight requests */
+    uint32_t max_batch;      /* requests per batch (0 = 256)                  */
+    uint32_t max_inflight;   /* batches on the GPU at once (0 = 2, max 16)    */
+    float load_factor;       /* resident join tables (0 = context default)    */
+    uint32_t plain;          /* 1 = one request at a time, operator API       */
+    uint32_t reserved[2];
+} mgv_server_config;
+
+typedef struct mgv_server_request {
+    uint32_t table;          /* from mgv_server_add_table                     */
+    uint32_t reserved;
+    const int32_t *probe_key, *probe_filter, *probe_group, *probe_value;  /* device */
+    uint64_t probe_rows;
+    int32_t filter_bound;
+    uint32_t max_groups;
+} mgv_server_request;
+
+typedef struct mgv_server_stats {
+    uint64_t submitted, completed, batches, rejected;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result on the host */
+    double mean_batch;
+    uint64_t resident_table_bytes, peak_bytes;
+} mgv_server_stats;
+
+typedef struct mgv_server mgv_server;
+
+mgv_status mgv_server_create(mgv_ctx *ctx, const mgv_server_config *cfg, mgv_server **out);
+/* Builds a hash table on (keys, payloads) and keeps it resident. */
+mgv_status mgv_server_add_table(mgv_server *s, const int32_t *keys, const int32_t *payloads, uint64_t rows,
+                                uint32_t *table_id);
+mgv_status mgv_server_submit(mgv_server *s, const mgv_server_request *r, uint64_t *ticket);
+/* Waits (bounded by timeout_ms) for a request; its groups sorted by group. */
+mgv_status mgv_server_wait(mgv_server *s, uint64_t ticket, uint32_t timeout_ms, mgv_group_row *out,
+                           uint64_t cap, uint64_t *rows, double *latency_ms);
+mgv_status mgv_server_stats_get(mgv_server *s, mgv_server_stats *out);
+mgv_status mgv_server_reset_stats(mgv_server *s);
+mgv_status mgv_server_destroy(mgv_server *s);
+
 /* ---- hash join without allocation ------------------------------------- */
 
 /* Largest build side mgv_hash_join_noalloc accepts. */

@@ -26,32 +26,14 @@
 #include "hash_table.cuh"
 #include "mgv_internal.h"
 
+#include <algorithm>
+
 namespace mgv {
 
 constexpr int kChainBlock = 256;
 constexpr int kChainWarps = kChainBlock / 32;
 constexpr int kRing = 256;
 
-struct ChainDev {
-    const int32_t* cols[MGV_MAX_COLS];
-    uint64_t n;
-    uint32_t ncols;
-    uint32_t nslots;                 // carried columns
-    int32_t slot_src[MGV_MAX_COLS];  // input column of each carried slot
-    uint32_t sel_col;
-    int32_t sel_bound;
-    int32_t probe_slot;
-    TableView table;
-    // terminal column references: carried slot, kBP (build payload) or -1
-    int32_t ref[MGV_MAX_COLS + 2];
-    uint32_t nref;
-    unsigned long long* acc;
-    GroupTableView gt;
-    uint32_t smem_groups;  // power of two, 0 = no shared table
-    SinkView sink;
-};
-
-constexpr int32_t kBP = 100;  // reference to the build payload
 
 // ---- device buffer pool: pop (swap-on-full for the sink) -------------------
 
@@ -209,31 +191,18 @@ __device__ __forceinline__ void group_add_warp(bool active, int32_t g, int32_t v
     }
 }
 
-// ---- the chain kernel ----------------------------------------------------------
+// ---- the chain: per-warp processing of a row range ------------------------------
 
-template <bool SEL, bool PROBE, bool UNIQUE, int TERM>
-__global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const uint32_t warp = threadIdx.x / 32, lane = lane_id();
-    // shared layout: [group sums u64 | ring int32 | group keys int32 | group counts u32]
-    SmemGroups sg{nullptr, nullptr, nullptr, 0};
-    unsigned long long* gsums = reinterpret_cast<unsigned long long*>(smem_raw);
-    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + (TERM == kTermGroupby ? a.smem_groups * 8 : 0));
-    if (TERM == kTermGroupby && a.smem_groups) {
-        sg.sums = gsums;
-        sg.keys = rings + kChainWarps * a.nslots * kRing;
-        sg.counts = reinterpret_cast<uint32_t*>(sg.keys + a.smem_groups);
-        sg.cap = a.smem_groups;
-        for (uint32_t i = threadIdx.x; i < sg.cap; i += kChainBlock) {
-            sg.keys[i] = kEmptyKey;
-            sg.sums[i] = 0;
-            sg.counts[i] = 0;
-        }
-        __syncthreads();
-    }
-    int32_t* ring = rings + (size_t)warp * a.nslots * kRing;
-    unsigned long long acnt = 0, asum = 0;
-
+// Windows of 128 rows of [row_lo, row_hi), this warp taking windows
+// win_first, win_first + win_stride, ...: select into the warp's ring,
+// push full vectors through the probe and the terminal, flush the last
+// partial vector.
+template <bool SEL, bool PROBE, int TERM>
+__device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, uint64_t row_lo, uint64_t row_hi,
+                                              uint64_t win_first, uint64_t win_stride, int32_t* ring,
+                                              const SmemGroups& sg, unsigned long long& acnt,
+                                              unsigned long long& asum, uint32_t* err) {
+    const uint32_t lane = lane_id();
     // value of terminal reference r for ring row rp and build payload bp
     auto val = [&](int32_t ref, uint32_t rp, int32_t bp) -> int32_t {
         return ref == kBP ? bp : ring[ref * kRing + rp];
@@ -314,7 +283,7 @@ __global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err
                             }
                         }
                         if (found) {
-                            if (UNIQUE) done = true;
+                            if (unique) done = true;
                         } else if (wb[6] != (uint32_t)kEmptyKey) {  // run continues
                             b = (b + 1 == a.table.nbuckets) ? 0u : b + 1;
                             slot = 0;
@@ -330,16 +299,14 @@ __global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err
         __syncwarp();
     };
 
-    const uint64_t nwin = (a.n + 127) / 128;
-    const uint64_t gwarp = (uint64_t)blockIdx.x * kChainWarps + warp;
-    const uint64_t nwarps = (uint64_t)gridDim.x * kChainWarps;
+    const uint64_t nwin = (row_hi - row_lo + 127) / 128;
     uint32_t head = 0, fill = 0;
-    for (uint64_t win = gwarp; win < nwin; win += nwarps) {
-        const uint64_t r0 = win * 128;
+    for (uint64_t win = win_first; win < nwin; win += win_stride) {
+        const uint64_t r0 = row_lo + win * 128;
 #pragma unroll 1
         for (int j = 0; j < 4; ++j) {
             const uint64_t row = r0 + j * 32 + lane;
-            bool pass = row < a.n;
+            bool pass = row < row_hi;
             if (SEL && pass) pass = __ldg(a.cols[a.sel_col] + row) <= a.sel_bound;
             const unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
@@ -355,18 +322,193 @@ __global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err
         }
     }
     if (fill) push_vector(head, fill);
+}
 
-    if (TERM == kTermAgg) block_accumulate2<kChainBlock>(acnt, asum, a.acc);
-    if (TERM == kTermGroupby && a.smem_groups) {
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < sg.cap; i += kChainBlock)
-            if (sg.keys[i] != kEmptyKey && sg.counts[i]) global_group_add(a.gt, sg.keys[i], sg.sums[i], sg.counts[i], err);
+__device__ __forceinline__ void smem_groups_init(const SmemGroups& sg) {
+    for (uint32_t i = threadIdx.x; i < sg.cap; i += blockDim.x) {
+        sg.keys[i] = kEmptyKey;
+        sg.sums[i] = 0;
+        sg.counts[i] = 0;
     }
 }
 
-template <bool SEL, bool PROBE, bool UNIQUE, int TERM>
+__device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const GroupTableView& gt, uint32_t* err) {
+    for (uint32_t i = threadIdx.x; i < sg.cap; i += blockDim.x)
+        if (sg.keys[i] != kEmptyKey && sg.counts[i]) global_group_add(gt, sg.keys[i], sg.sums[i], sg.counts[i], err);
+}
+
+template <bool SEL, bool PROBE, int TERM>
+__global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t warp = threadIdx.x / 32;
+    // shared layout: [group sums u64 | rings int32 | group keys int32 | group counts u32]
+    SmemGroups sg{nullptr, nullptr, nullptr, 0};
+    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + (TERM == kTermGroupby ? a.smem_groups * 8 : 0));
+    if (TERM == kTermGroupby && a.smem_groups) {
+        sg.sums = reinterpret_cast<unsigned long long*>(smem_raw);
+        sg.keys = rings + kChainWarps * a.nslots * kRing;
+        sg.counts = reinterpret_cast<uint32_t*>(sg.keys + a.smem_groups);
+        sg.cap = a.smem_groups;
+        smem_groups_init(sg);
+        __syncthreads();
+    }
+    unsigned long long acnt = 0, asum = 0;
+    chain_windows<SEL, PROBE, TERM>(a, a.unique != 0, 0, a.n, (uint64_t)blockIdx.x * kChainWarps + warp,
+                                    (uint64_t)gridDim.x * kChainWarps, rings + (size_t)warp * a.nslots * kRing, sg,
+                                    acnt, asum, err);
+    if (TERM == kTermAgg) block_accumulate2<kChainBlock>(acnt, asum, a.acc);
+    if (TERM == kTermGroupby && a.smem_groups) {
+        __syncthreads();
+        smem_groups_flush(sg, a.gt, err);
+    }
+}
+
+// ---- batched queries ------------------------------------------------------------
+
+constexpr int kBatchSlots = 3;          // key, group, value
+constexpr uint32_t kBatchSmemGroups = 4096;
+
+// Probe phase of a batch: every CTA takes a contiguous run of (query, rows)
+// items in query order, so it stays on one query for many items; queries
+// with at most kBatchSmemGroups/2 groups aggregate in the CTA's shared table,
+// flushed to the query's global table when the CTA moves to another query.
+__global__ void __launch_bounds__(kChainBlock) k_batch_probe(const ChainDev* __restrict__ qs,
+                                                             const BatchItem* __restrict__ items, uint32_t nitems,
+                                                             uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t warp = threadIdx.x / 32;
+    SmemGroups full_sg;
+    full_sg.sums = reinterpret_cast<unsigned long long*>(smem_raw);
+    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + kBatchSmemGroups * 8);
+    full_sg.keys = rings + kChainWarps * kBatchSlots * kRing;
+    full_sg.counts = reinterpret_cast<uint32_t*>(full_sg.keys + kBatchSmemGroups);
+    full_sg.cap = kBatchSmemGroups;
+    const SmemGroups no_sg{nullptr, nullptr, nullptr, 0};
+
+    const uint32_t it0 = (uint32_t)((uint64_t)blockIdx.x * nitems / gridDim.x);
+    const uint32_t it1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * nitems / gridDim.x);
+    int64_t cur = -1;
+    bool cur_smem = false;
+    unsigned long long acnt = 0, asum = 0;
+    for (uint32_t it = it0; it < it1; ++it) {
+        const BatchItem item = items[it];
+        if ((int64_t)item.q != cur) {
+            if (cur_smem) {
+                __syncthreads();
+                smem_groups_flush(full_sg, qs[cur].gt, err);
+            }
+            cur = item.q;
+            cur_smem = qs[cur].smem_groups != 0;
+            if (cur_smem) {
+                __syncthreads();
+                smem_groups_init(full_sg);
+            }
+            __syncthreads();
+        }
+        const ChainDev& a = qs[item.q];
+        const bool unique = a.table.meta[3] == 0;
+        chain_windows<true, true, kTermGroupby>(a, unique, item.lo, item.hi, warp, kChainWarps,
+                                                rings + (size_t)warp * kBatchSlots * kRing,
+                                                cur_smem ? full_sg : no_sg, acnt, asum, err);
+    }
+    if (cur_smem) {
+        __syncthreads();
+        smem_groups_flush(full_sg, qs[cur].gt, err);
+    }
+}
+
+// Build phase of a batch: contiguous runs of (query, rows) items; every row
+// is inserted into its query's table.
+__global__ void __launch_bounds__(kChainBlock) k_batch_build(const BatchBuild* __restrict__ bs,
+                                                             const BatchItem* __restrict__ items, uint32_t nitems,
+                                                             uint32_t* err) {
+    const uint32_t it0 = (uint32_t)((uint64_t)blockIdx.x * nitems / gridDim.x);
+    const uint32_t it1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * nitems / gridDim.x);
+    for (uint32_t it = it0; it < it1; ++it) {
+        const BatchItem item = items[it];
+        const BatchBuild& b = bs[item.q];
+        bool dup = false;
+        uint32_t inserted = 0;
+        for (uint64_t i = item.lo + threadIdx.x; i < item.hi; i += kChainBlock) {
+            bool ok;
+            table_insert(b.table, __ldg(b.keys + i), b.pays ? __ldg(b.pays + i) : 0, err, dup, ok);
+            inserted += ok;
+        }
+        const unsigned long long tot = warp_sum_u64(inserted);
+        const unsigned any_dup = __any_sync(0xffffffffu, dup);
+        if (lane_id() == 0) {
+            if (tot) atomicAdd(b.table.meta + 2, tot);
+            if (any_dup) atomicOr(b.table.meta + 3, 1ull);
+        }
+    }
+}
+
+// Packs each query's groups into its output region (unsorted) and counts them.
+__global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchItem* __restrict__ items,
+                                uint32_t nitems, uint32_t* err) {
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const BatchItem item = items[it];
+        const BatchOut& o = outs[item.q];
+        for (uint64_t i = item.lo + threadIdx.x; i < item.hi; i += blockDim.x) {
+            const bool special = i == o.gt.cap;  // one extra index for the group INT32_MIN
+            const int32_t k = special ? kEmptyKey : o.gt.keys[i];
+            const unsigned long long c = special ? o.gt.special[1] : o.gt.counts[i];
+            if ((!special && k == kEmptyKey) || c == 0) continue;
+            const uint32_t pos = atomicAdd(o.count, 1u);
+            if (pos >= o.capacity) {
+                set_error(err, kDevOverflow, 30);
+                continue;
+            }
+            mgv_group_row r;
+            r.group = k;
+            r.pad = 0;
+            r.sum = (int64_t)(special ? o.gt.special[0] : o.gt.sums[i]);
+            r.count = (int64_t)c;
+            o.rows[pos] = r;
+        }
+    }
+}
+
+cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
+                         const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
+                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, cudaStream_t s,
+                         Context* ctx) {
+    const int sms = ctx->prop.multiProcessorCount;
+    if (n_build) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_build, kChainBlock, 0);
+        const int grid = (int)std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, n_build);
+        k_batch_build<<<grid, kChainBlock, 0, s>>>(d_builds, build_items, n_build, ctx->d_err);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (n_probe) {
+        const size_t smem = (size_t)kChainWarps * kBatchSlots * kRing * sizeof(int32_t) + (size_t)kBatchSmemGroups * 16;
+        cudaError_t e = cudaFuncSetAttribute(k_batch_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_probe, kChainBlock, smem);
+        per_sm = std::max(per_sm, 1);
+        if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+        const int grid = (int)std::min<uint64_t>((uint64_t)per_sm * sms, n_probe);
+        k_batch_probe<<<grid, kChainBlock, smem, s>>>(d_qs, probe_items, n_probe, ctx->d_err);
+        ctx->launches++;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (n_compact) {
+        const int grid = (int)std::min<uint64_t>((uint64_t)sms * 8, n_compact);
+        k_batch_compact<<<grid, 256, 0, s>>>(d_outs, compact_items, n_compact, ctx->d_err);
+        ctx->launches++;
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
+}
+
+template <bool SEL, bool PROBE, int TERM>
 static cudaError_t launch_chain_t(const ChainDev& d, size_t smem, uint64_t n, cudaStream_t s, Context* ctx) {
-    auto k = k_chain<SEL, PROBE, UNIQUE, TERM>;
+    auto k = k_chain<SEL, PROBE, TERM>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -382,13 +524,10 @@ static cudaError_t launch_chain_t(const ChainDev& d, size_t smem, uint64_t n, cu
 template <int TERM>
 static cudaError_t launch_chain_term(const ChainArgs& a, const ChainDev& d, size_t smem, cudaStream_t s, Context* ctx) {
     if (!a.has_probe)
-        return a.has_sel ? launch_chain_t<true, false, false, TERM>(d, smem, a.n, s, ctx)
-                         : launch_chain_t<false, false, false, TERM>(d, smem, a.n, s, ctx);
-    if (a.unique)
-        return a.has_sel ? launch_chain_t<true, true, true, TERM>(d, smem, a.n, s, ctx)
-                         : launch_chain_t<false, true, true, TERM>(d, smem, a.n, s, ctx);
-    return a.has_sel ? launch_chain_t<true, true, false, TERM>(d, smem, a.n, s, ctx)
-                     : launch_chain_t<false, true, false, TERM>(d, smem, a.n, s, ctx);
+        return a.has_sel ? launch_chain_t<true, false, TERM>(d, smem, a.n, s, ctx)
+                         : launch_chain_t<false, false, TERM>(d, smem, a.n, s, ctx);
+    return a.has_sel ? launch_chain_t<true, true, TERM>(d, smem, a.n, s, ctx)
+                     : launch_chain_t<false, true, TERM>(d, smem, a.n, s, ctx);
 }
 
 cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx) {
@@ -400,6 +539,7 @@ cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx) {
     d.sel_col = a.sel_col;
     d.sel_bound = a.sel_bound;
     d.table = a.table;
+    d.unique = a.unique ? 1u : 0u;
     d.acc = a.acc;
     d.gt = a.gt;
     d.sink = a.sink;

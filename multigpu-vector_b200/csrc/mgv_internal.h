@@ -111,6 +111,8 @@ struct Context {
     unsigned long long* h_stage = nullptr;
     std::atomic<uint64_t> launches{0};
     mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, 4096u, {0u, 0u}};
+    mgv_batch_config batch_tuned{};  // the batch autotuner's last choice
+    bool has_batch_tuned = false;
     std::mutex mu;
 };
 
@@ -209,6 +211,52 @@ struct ChainArgs {
     SinkView sink;
 };
 cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx);
+
+// Device-side parameters of one chain (one query of a batch).
+struct ChainDev {
+    const int32_t* cols[MGV_MAX_COLS];
+    uint64_t n;
+    uint32_t ncols;
+    uint32_t nslots;                 // carried columns
+    int32_t slot_src[MGV_MAX_COLS];  // input column of each carried slot
+    uint32_t sel_col;
+    int32_t sel_bound;
+    int32_t probe_slot;
+    uint32_t unique;  // the table has no duplicate keys: a probe stops at its match
+    TableView table;
+    // terminal column references: carried slot, kBP (build payload) or -1
+    int32_t ref[MGV_MAX_COLS + 2];
+    uint32_t nref;
+    unsigned long long* acc;
+    GroupTableView gt;
+    uint32_t smem_groups;  // power of two, 0 = no shared table
+    SinkView sink;
+};
+
+constexpr int32_t kBP = 100;  // terminal reference to the build payload
+
+// Batched execution (chain.cu kernels, batch.cu host side).
+struct BatchItem {  // rows [lo, hi) of query q
+    uint32_t q;
+    uint32_t pad;
+    uint64_t lo, hi;
+};
+struct BatchBuild {  // build side of a query
+    const int32_t* keys;
+    const int32_t* pays;
+    TableView table;
+};
+struct BatchOut {  // packed result region of a query
+    GroupTableView gt;
+    mgv_group_row* rows;
+    uint32_t* count;
+    uint32_t capacity;
+    uint32_t pad;
+};
+cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
+                         const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
+                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, cudaStream_t s,
+                         Context* ctx);
 
 // partition.cu
 cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,

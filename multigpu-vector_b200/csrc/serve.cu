@@ -1,0 +1,486 @@
+// serve.cu -- a query server with continuous batching.
+//
+// Build tables are registered once and stay resident.  Clients submit
+// select -> join -> group-by requests against them at any time; a scheduler
+// thread admits pending requests in arrival order while the device memory
+// budget allows (group table + packed result region per request), launches
+// them as one batch (one persistent probe kernel over (query, rows) items,
+// then the result packing and one copy to pinned host memory) on a free
+// stream, and keeps up to max_inflight batches on the GPU at once, so
+// requests that arrive while others run are admitted as soon as a stream
+// and memory free up and their work overlaps on the device.  Completion is
+// observed through CUDA events; latency runs from submit to the moment the
+// scheduler sees the batch's results on the host.
+//
+// With plain = 1 the server instead runs requests one at a time through the
+// operator API (select -> hash_probe -> groupby on the resident table): the
+// per-query baseline under the same arrival trace.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "device_common.cuh"
+#include "mgv_internal.h"
+
+using namespace mgv;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Request {
+    uint64_t ticket = 0;
+    mgv_server_request r{};
+    Clock::time_point t_submit;
+    double latency_ms = 0.0;
+    mgv_status status = MGV_OK;
+    bool done = false;
+    std::vector<mgv_group_row> rows;
+    size_t bytes = 0;  // admission charge
+};
+
+struct Inflight {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<std::shared_ptr<Request>> reqs;
+    void* dmem = nullptr;
+    size_t charge = 0;
+    mgv_group_row* h_rows = nullptr;  // pinned
+    size_t h_cap = 0;                 // rows
+    uint32_t* h_counts = nullptr;     // pinned, inside h_rows allocation
+    std::vector<uint64_t> offs;
+    bool busy = false;
+};
+
+uint32_t group_cap(uint32_t max_groups) {
+    uint32_t cap = 64;
+    while (cap < 2u * max_groups) cap <<= 1;
+    return cap;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t request_bytes(const mgv_server_request& r) {
+    const uint64_t cap = group_cap(r.max_groups);
+    return align256(cap * 20 + 16) + align256((size_t)r.max_groups * sizeof(mgv_group_row)) + 512;
+}
+
+}  // namespace
+
+struct mgv_server {
+    mgv_ctx* ctx = nullptr;
+    mgv_server_config cfg{};
+    std::vector<mgv_op*> tables;  // resident hash_build operators
+    size_t table_bytes = 0;
+    std::mutex mu;
+    std::condition_variable cv;       // scheduler wake-up
+    std::condition_variable done_cv;  // request completion
+    std::deque<std::shared_ptr<Request>> pending;
+    std::map<uint64_t, std::shared_ptr<Request>> by_ticket;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    size_t used = 0, peak = 0;
+    std::vector<Inflight> slots;
+    std::thread th;
+    // stats
+    std::vector<double> latencies;
+    uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0;
+    // plain mode: group-by operators (device tables) reused per max_groups
+    std::map<uint32_t, mgv_op*> plain_gb;
+};
+
+namespace {
+
+void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
+    q->status = st;
+    q->latency_ms = std::chrono::duration<double, std::milli>(Clock::now() - q->t_submit).count();
+    q->done = true;
+    S->latencies.push_back(q->latency_ms);
+    S->completed++;
+}
+
+// Launch one batch of admitted requests on slot `sl` (scheduler thread, lock held).
+mgv_status launch(mgv_server* S, Inflight& sl) {
+    Context* ctx = S->ctx;
+    const uint32_t nq = (uint32_t)sl.reqs.size();
+    // device layout: [group keys | zeroed: sums counts specials | counts | rows | qs | outs | items]
+    size_t off = 0;
+    std::vector<size_t> gk(nq), gs(nq), gc(nq), sp(nq);
+    std::vector<uint32_t> caps(nq);
+    uint64_t slots = 0, rows = 0;
+    for (uint32_t i = 0; i < nq; ++i) {
+        caps[i] = group_cap(sl.reqs[i]->r.max_groups);
+        gk[i] = off;
+        off += 4ull * caps[i];
+        slots += caps[i];
+    }
+    off = align256(off);
+    const size_t zero_begin = off;
+    for (uint32_t i = 0; i < nq; ++i) {
+        gs[i] = off; off += 8ull * caps[i];
+        gc[i] = off; off += 8ull * caps[i];
+        sp[i] = off; off += 16;
+    }
+    const size_t zero_end = off;
+    off = align256(off);
+    const size_t counts_off = off;
+    off = align256(off + 4ull * nq);
+    sl.offs.resize(nq);
+    for (uint32_t i = 0; i < nq; ++i) { sl.offs[i] = rows; rows += sl.reqs[i]->r.max_groups; }
+    const size_t rows_off = off;
+    off = align256(off + sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1));
+    std::vector<BatchItem> pi, ci;
+    const uint64_t item_rows = 32768;
+    for (uint32_t i = 0; i < nq; ++i) {
+        for (uint64_t lo = 0; lo < sl.reqs[i]->r.probe_rows; lo += item_rows)
+            pi.push_back(BatchItem{i, 0, lo, std::min<uint64_t>(sl.reqs[i]->r.probe_rows, lo + item_rows)});
+        for (uint64_t lo = 0; lo <= caps[i]; lo += 65536)
+            ci.push_back(BatchItem{i, 0, lo, std::min<uint64_t>((uint64_t)caps[i] + 1, lo + 65536)});
+    }
+    const size_t qs_off = off;
+    off = align256(off + sizeof(ChainDev) * nq);
+    const size_t outs_off = off;
+    off = align256(off + sizeof(BatchOut) * nq);
+    const size_t pi_off = off;
+    off = align256(off + sizeof(BatchItem) * std::max<size_t>(pi.size(), 1));
+    const size_t ci_off = off;
+    off = align256(off + sizeof(BatchItem) * std::max<size_t>(ci.size(), 1));
+
+    MGV_CUDA_TRY(cudaMallocAsync(&sl.dmem, off, sl.stream));
+    unsigned char* A = static_cast<unsigned char*>(sl.dmem);
+    // pinned landing zone: rows + counts
+    const size_t need_rows = std::max<uint64_t>(rows, 1);
+    if (sl.h_cap < need_rows || !sl.h_rows) {
+        if (sl.h_rows) cudaFreeHost(sl.h_rows);
+        sl.h_cap = std::max<size_t>(need_rows, 2 * sl.h_cap);
+        MGV_CUDA_TRY(cudaMallocHost(&sl.h_rows, sizeof(mgv_group_row) * sl.h_cap + 4ull * (S->cfg.max_batch + 4)));
+        sl.h_counts = reinterpret_cast<uint32_t*>(sl.h_rows + sl.h_cap);
+    }
+    std::vector<ChainDev> hq(nq);
+    std::vector<BatchOut> ho(nq);
+    for (uint32_t i = 0; i < nq; ++i) {
+        const mgv_server_request& r = sl.reqs[i]->r;
+        GroupTableView g{};
+        g.keys = reinterpret_cast<int32_t*>(A + gk[i]);
+        g.sums = reinterpret_cast<unsigned long long*>(A + gs[i]);
+        g.counts = reinterpret_cast<unsigned long long*>(A + gc[i]);
+        g.special = reinterpret_cast<unsigned long long*>(A + sp[i]);
+        g.cap = caps[i];
+        ChainDev& c = hq[i];
+        c = ChainDev{};
+        c.cols[0] = r.probe_key;
+        c.cols[1] = r.probe_filter;
+        c.cols[2] = r.probe_group;
+        c.cols[3] = r.probe_value;
+        c.n = r.probe_rows;
+        c.ncols = 4;
+        c.nslots = 3;
+        c.slot_src[0] = 0;
+        c.slot_src[1] = 2;
+        c.slot_src[2] = 3;
+        c.sel_col = 1;
+        c.sel_bound = r.filter_bound;
+        c.probe_slot = 0;
+        c.table = S->tables[r.table]->table;
+        c.ref[0] = 1;
+        c.ref[1] = 2;
+        c.nref = 2;
+        c.gt = g;
+        c.smem_groups = caps[i] <= 4096 ? 1u : 0u;
+        ho[i] = BatchOut{g, reinterpret_cast<mgv_group_row*>(A + rows_off) + sl.offs[i],
+                         reinterpret_cast<uint32_t*>(A + counts_off) + i, r.max_groups, 0};
+    }
+    cudaStream_t s = sl.stream;
+    // host staging of descriptors must outlive the copies: pageable copies
+    // are staged by the driver before cudaMemcpyAsync returns
+    MGV_CUDA_TRY(cudaMemcpyAsync(A + qs_off, hq.data(), sizeof(ChainDev) * nq, cudaMemcpyHostToDevice, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(A + outs_off, ho.data(), sizeof(BatchOut) * nq, cudaMemcpyHostToDevice, s));
+    if (!pi.empty())
+        MGV_CUDA_TRY(cudaMemcpyAsync(A + pi_off, pi.data(), sizeof(BatchItem) * pi.size(), cudaMemcpyHostToDevice, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(A + ci_off, ci.data(), sizeof(BatchItem) * ci.size(), cudaMemcpyHostToDevice, s));
+    MGV_CUDA_TRY(launch_fill_i32(reinterpret_cast<int32_t*>(A), slots, kEmptyKey, s, ctx));
+    MGV_CUDA_TRY(cudaMemsetAsync(A + zero_begin, 0, zero_end - zero_begin, s));
+    MGV_CUDA_TRY(cudaMemsetAsync(A + counts_off, 0, 4ull * nq, s));
+    MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), nullptr,
+                              reinterpret_cast<BatchOut*>(A + outs_off), nullptr, 0,
+                              reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(),
+                              reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, s, ctx));
+    MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
+                                 cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaFreeAsync(sl.dmem, s));
+    MGV_CUDA_TRY(cudaEventRecord(sl.done, s));
+    sl.busy = true;
+    S->batches++;
+    S->batched_queries += nq;
+    return MGV_OK;
+}
+
+// Results of a finished batch (lock held).
+void harvest(mgv_server* S, Inflight& sl) {
+    for (size_t i = 0; i < sl.reqs.size(); ++i) {
+        auto& q = sl.reqs[i];
+        const uint32_t n = std::min<uint32_t>(sl.h_counts[i], q->r.max_groups);
+        q->rows.assign(sl.h_rows + sl.offs[i], sl.h_rows + sl.offs[i] + n);
+        std::sort(q->rows.begin(), q->rows.end(),
+                  [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+        complete(S, q, sl.h_counts[i] > q->r.max_groups ? MGV_ENOMEM : MGV_OK);
+        S->used -= q->bytes;
+    }
+    sl.reqs.clear();
+    sl.busy = false;
+    sl.dmem = nullptr;
+}
+
+// Plain mode: one request through the operator API (lock not held).
+mgv_status run_plain(mgv_server* S, Request& q) {
+    const mgv_server_request& r = q.r;
+    mgv_ctx* ctx = S->ctx;
+    mgv_op *gb = nullptr, *probe = nullptr, *sel = nullptr;
+    mgv_status st = MGV_OK;
+    auto it = S->plain_gb.find(r.max_groups);
+    if (it != S->plain_gb.end()) {
+        gb = it->second;
+    } else {
+        mgv_groupby_desc gd{2, 3, r.max_groups, 0};
+        st = mgv_op_create_groupby(ctx, &gd, &gb);
+        if (st != MGV_OK) return st;
+        S->plain_gb[r.max_groups] = gb;
+    }
+    mgv_hash_probe_desc pd{0, 0, S->tables[r.table]};
+    if (st == MGV_OK) st = mgv_op_create_hash_probe(ctx, &pd, gb, &probe);
+    mgv_select_desc sd{1, r.filter_bound};
+    if (st == MGV_OK) st = mgv_op_create_select(ctx, &sd, probe, &sel);
+    const int32_t* cols[4] = {r.probe_key, r.probe_filter, r.probe_group, r.probe_value};
+    if (st == MGV_OK) st = mgv_op_open(sel, nullptr);
+    if (st == MGV_OK) st = mgv_op_consume_columns(sel, cols, 4, r.probe_rows, nullptr);
+    if (st == MGV_OK) st = mgv_op_close(sel, nullptr);
+    if (st == MGV_OK) {
+        size_t need = 0;
+        mgv_op_result(gb, nullptr, 0, &need);
+        q.rows.resize(need / sizeof(mgv_group_row));
+        mgv_op_result(gb, q.rows.data(), need, nullptr);
+    }
+    mgv_op_destroy(sel);
+    mgv_op_destroy(probe);
+    return st;
+}
+
+void scheduler(mgv_server* S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (true) {
+        if (S->cfg.plain) {
+            S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+            if (S->stop && S->pending.empty()) break;
+            auto q = S->pending.front();
+            S->pending.pop_front();
+            lk.unlock();
+            const mgv_status st = run_plain(S, *q);
+            lk.lock();
+            complete(S, q, st);
+            S->done_cv.notify_all();
+            continue;
+        }
+        // 1. harvest finished batches
+        bool any_busy = false;
+        for (auto& sl : S->slots) {
+            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) {
+                harvest(S, sl);
+                S->done_cv.notify_all();
+            }
+            any_busy |= sl.busy;
+        }
+        // 2. admit pending requests into a free slot
+        Inflight* free_slot = nullptr;
+        for (auto& sl : S->slots)
+            if (!sl.busy) { free_slot = &sl; break; }
+        if (free_slot && !S->pending.empty()) {
+            const size_t budget = S->cfg.memory_budget > S->table_bytes ? S->cfg.memory_budget - S->table_bytes : 0;
+            while (!S->pending.empty() && free_slot->reqs.size() < S->cfg.max_batch) {
+                auto& q = S->pending.front();
+                if (q->bytes > budget) {  // can never fit
+                    auto r = q;
+                    S->pending.pop_front();
+                    S->rejected++;
+                    complete(S, r, MGV_ENOMEM);
+                    S->done_cv.notify_all();
+                    continue;
+                }
+                if (S->used + q->bytes > budget) break;  // wait for memory to free up
+                S->used += q->bytes;
+                S->peak = std::max(S->peak, S->used + S->table_bytes);
+                free_slot->reqs.push_back(q);
+                S->pending.pop_front();
+            }
+            if (!free_slot->reqs.empty()) {
+                const mgv_status st = launch(S, *free_slot);
+                if (st != MGV_OK) {
+                    for (auto& q : free_slot->reqs) { S->used -= q->bytes; complete(S, q, st); }
+                    free_slot->reqs.clear();
+                    free_slot->busy = false;
+                    S->done_cv.notify_all();
+                }
+                continue;
+            }
+        }
+        if (S->stop && S->pending.empty() && !any_busy) break;
+        if (any_busy)
+            S->cv.wait_for(lk, std::chrono::microseconds(20));  // poll the GPU
+        else
+            S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_server** out) {
+    if (!ctx || !cfg || !out) return fail(MGV_EINVAL, "NULL argument");
+    *out = nullptr;
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    mgv_server* S = new (std::nothrow) mgv_server();
+    if (!S) return fail(MGV_ENOMEM, "host allocation");
+    S->ctx = ctx;
+    S->cfg = *cfg;
+    if (S->cfg.max_batch == 0) S->cfg.max_batch = 256;
+    if (S->cfg.max_inflight == 0) S->cfg.max_inflight = 2;
+    if (S->cfg.max_inflight > 16) S->cfg.max_inflight = 16;
+    if (S->cfg.load_factor == 0.0f) S->cfg.load_factor = ctx->tuning.default_load_factor;
+    S->slots.resize(S->cfg.max_inflight);
+    for (auto& sl : S->slots) {
+        cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "mgv_server_create");
+    }
+    S->th = std::thread(scheduler, S);
+    *out = S;
+    return MGV_OK;
+}
+
+mgv_status mgv_server_add_table(mgv_server* S, const int32_t* keys, const int32_t* payloads, uint64_t rows,
+                                uint32_t* table_id) {
+    if (!S || (!keys && rows) || !table_id) return fail(MGV_EINVAL, "NULL argument");
+    mgv_hash_build_desc d{0, payloads ? 1 : -1, std::max<uint64_t>(rows, 1), S->cfg.load_factor, 0, 0, 0};
+    mgv_op* hb = nullptr;
+    mgv_status st = mgv_op_create_hash_build(S->ctx, &d, &hb);
+    const int32_t* cols[2] = {keys, payloads};
+    if (st == MGV_OK) st = mgv_op_open(hb, nullptr);
+    if (st == MGV_OK) st = mgv_op_consume_columns(hb, cols, payloads ? 2 : 1, rows, nullptr);
+    if (st == MGV_OK) st = mgv_op_close(hb, nullptr);
+    if (st != MGV_OK) {
+        if (hb) mgv_op_destroy(hb);
+        return st;
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->tables.push_back(hb);
+    S->table_bytes += hb->table_bytes + sizeof(int32_t) * hb->table.side_cap;
+    *table_id = (uint32_t)(S->tables.size() - 1);
+    return MGV_OK;
+}
+
+mgv_status mgv_server_submit(mgv_server* S, const mgv_server_request* r, uint64_t* ticket) {
+    if (!S || !r || !ticket) return fail(MGV_EINVAL, "NULL argument");
+    if (r->max_groups == 0 || r->max_groups > (1u << 28)) return fail(MGV_EINVAL, "max_groups out of range");
+    if (r->probe_rows && (!r->probe_key || !r->probe_filter || !r->probe_group || !r->probe_value))
+        return fail(MGV_EINVAL, "NULL probe column");
+    auto q = std::make_shared<Request>();
+    q->r = *r;
+    q->bytes = request_bytes(*r);
+    q->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (r->table >= S->tables.size()) return fail(MGV_EINVAL, "no such table");
+        if (S->stop) return fail(MGV_ESTATE, "server is stopping");
+        q->ticket = S->next_ticket++;
+        S->by_ticket[q->ticket] = q;
+        S->pending.push_back(q);
+        S->submitted++;
+    }
+    S->cv.notify_all();
+    *ticket = q->ticket;
+    return MGV_OK;
+}
+
+mgv_status mgv_server_wait(mgv_server* S, uint64_t ticket, uint32_t timeout_ms, mgv_group_row* out, uint64_t cap,
+                           uint64_t* rows, double* latency_ms) {
+    if (!S) return fail(MGV_EINVAL, "server is NULL");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->by_ticket.find(ticket);
+    if (it == S->by_ticket.end()) return fail(MGV_EINVAL, "unknown ticket");
+    auto q = it->second;
+    if (!S->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; }))
+        return fail(MGV_ETIMEDOUT, "request not finished");
+    if (rows) *rows = q->rows.size();
+    if (latency_ms) *latency_ms = q->latency_ms;
+    if (out) std::copy(q->rows.begin(), q->rows.begin() + std::min<uint64_t>(cap, q->rows.size()), out);
+    S->by_ticket.erase(it);
+    if (q->status != MGV_OK) return fail(q->status, "request failed");
+    return MGV_OK;
+}
+
+mgv_status mgv_server_stats_get(mgv_server* S, mgv_server_stats* out) {
+    if (!S || !out) return fail(MGV_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *out = mgv_server_stats{};
+    out->submitted = S->submitted;
+    out->completed = S->completed;
+    out->batches = S->batches;
+    out->rejected = S->rejected;
+    out->mean_batch = S->batches ? (double)S->batched_queries / S->batches : 0.0;
+    out->resident_table_bytes = S->table_bytes;
+    out->peak_bytes = S->peak;
+    if (!S->latencies.empty()) {
+        std::vector<double> v = S->latencies;
+        std::sort(v.begin(), v.end());
+        auto pct = [&](double p) { return v[std::min<size_t>(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))]; };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        out->max_ms = v.back();
+        double s = 0;
+        for (double x : v) s += x;
+        out->mean_ms = s / v.size();
+    }
+    return MGV_OK;
+}
+
+mgv_status mgv_server_reset_stats(mgv_server* S) {
+    if (!S) return fail(MGV_EINVAL, "server is NULL");
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->latencies.clear();
+    S->submitted = S->completed = S->batches = S->rejected = S->batched_queries = 0;
+    S->peak = S->used + S->table_bytes;
+    return MGV_OK;
+}
+
+mgv_status mgv_server_destroy(mgv_server* S) {
+    if (!S) return MGV_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv.notify_all();
+    if (S->th.joinable()) S->th.join();
+    cudaSetDevice(S->ctx->device);
+    for (auto& sl : S->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        if (sl.h_rows) cudaFreeHost(sl.h_rows);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
+    for (mgv_op* t : S->tables) mgv_op_destroy(t);
+    delete S;
+    return MGV_OK;
+}
+
+}  // extern "C"

@@ -101,6 +101,40 @@ class PartitionDesc(ctypes.Structure):
                 ("max_rows", c_uint64)]
 
 
+class QueryDesc(ctypes.Structure):
+    _fields_ = [("build_keys", c_void_p), ("build_payloads", c_void_p), ("build_rows", c_uint64),
+                ("probe_key", c_void_p), ("probe_filter", c_void_p), ("probe_group", c_void_p),
+                ("probe_value", c_void_p), ("probe_rows", c_uint64), ("filter_bound", c_int32),
+                ("max_groups", c_uint32)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("load_factor", c_float), ("build_item_rows", c_uint32), ("probe_item_rows", c_uint32),
+                ("probe_ctas_per_sm", c_uint32), ("use_graph", c_uint32), ("reserved", c_uint32 * 3)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("arena_bytes", c_uint64), ("queries", c_uint32), ("build_items", c_uint32),
+                ("probe_items", c_uint32), ("graph", c_uint32), ("last_run_ms", c_double)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("memory_budget", c_uint64), ("max_batch", c_uint32), ("max_inflight", c_uint32),
+                ("load_factor", c_float), ("plain", c_uint32), ("reserved", c_uint32 * 2)]
+
+
+class ServerRequest(ctypes.Structure):
+    _fields_ = [("table", c_uint32), ("reserved", c_uint32), ("probe_key", c_void_p), ("probe_filter", c_void_p),
+                ("probe_group", c_void_p), ("probe_value", c_void_p), ("probe_rows", c_uint64),
+                ("filter_bound", c_int32), ("max_groups", c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("batches", c_uint64), ("rejected", c_uint64),
+                ("p50_ms", c_double), ("p99_ms", c_double), ("mean_ms", c_double), ("max_ms", c_double),
+                ("mean_batch", c_double), ("resident_table_bytes", c_uint64), ("peak_bytes", c_uint64)]
+
+
 class SinkDesc(ctypes.Structure):
     _fields_ = [("pool", c_void_p), ("max_buffers", c_uint32), ("reserved", c_uint32)]
 
@@ -161,6 +195,21 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_gen_perm": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
         "mgv_gen_probe_keys": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint64, c_uint64, c_uint32,
                                     c_int64, c_uint64, POINTER(c_uint64), c_void_p]),
+        "mgv_batch_create": (st, [c_void_p, POINTER(QueryDesc), c_uint32, POINTER(BatchConfig), POINTER(c_void_p)]),
+        "mgv_batch_run": (st, [c_void_p, c_void_p]),
+        "mgv_batch_run_plain": (st, [c_void_p, c_void_p]),
+        "mgv_batch_result": (st, [c_void_p, c_uint32, c_int, c_void_p, c_uint64, POINTER(c_uint64)]),
+        "mgv_batch_stats_get": (st, [c_void_p, POINTER(BatchStats)]),
+        "mgv_batch_destroy": (st, [c_void_p]),
+        "mgv_batch_autotune": (st, [c_void_p, POINTER(QueryDesc), c_uint32, POINTER(BatchConfig)]),
+        "mgv_server_create": (st, [c_void_p, POINTER(ServerConfig), POINTER(c_void_p)]),
+        "mgv_server_add_table": (st, [c_void_p, c_void_p, c_void_p, c_uint64, POINTER(c_uint32)]),
+        "mgv_server_submit": (st, [c_void_p, POINTER(ServerRequest), POINTER(c_uint64)]),
+        "mgv_server_wait": (st, [c_void_p, c_uint64, c_uint32, c_void_p, c_uint64, POINTER(c_uint64),
+                                 POINTER(c_double)]),
+        "mgv_server_stats_get": (st, [c_void_p, POINTER(ServerStats)]),
+        "mgv_server_reset_stats": (st, [c_void_p]),
+        "mgv_server_destroy": (st, [c_void_p]),
         "mgv_hash_join_noalloc": (st, [c_int, c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,
                                        c_void_p, c_void_p]),
         "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
@@ -419,6 +468,106 @@ class Op:
     def destroy(self) -> None:
         if self.h:
             load().mgv_op_destroy(self.h)
+            self.h = None
+
+
+def query_desc(build_keys, build_rows, probe_key, probe_filter, probe_group, probe_value, probe_rows,
+               filter_bound, max_groups, build_payloads=None) -> QueryDesc:
+    p = lambda x: None if x is None else _ptr(x)
+    return QueryDesc(p(build_keys), p(build_payloads), build_rows, p(probe_key), p(probe_filter), p(probe_group),
+                     p(probe_value), probe_rows, filter_bound, max_groups)
+
+
+class Batch:
+    """mgv_batch: many select -> join -> group-by queries run together."""
+
+    def __init__(self, ctx: Context, queries, config: BatchConfig | None = None, keep=None):
+        self.ctx = ctx
+        self.keep = keep  # device tensors the descriptors point into
+        arr = (QueryDesc * max(1, len(queries)))(*queries)
+        self.nq = len(queries)
+        h = c_void_p()
+        _call("mgv_batch_create", ctx.h, arr, self.nq, byref(config) if config is not None else None, byref(h))
+        self.h = h
+
+    def run(self, stream=None) -> None:
+        _call("mgv_batch_run", self.h, _stream(stream))
+
+    def run_plain(self, stream=None) -> None:
+        _call("mgv_batch_run_plain", self.h, _stream(stream))
+
+    def result(self, q: int, plain: bool = False):
+        n = c_uint64()
+        _call("mgv_batch_result", self.h, q, int(plain), None, 0, byref(n))
+        arr = (GroupRow * max(1, n.value))()
+        _call("mgv_batch_result", self.h, q, int(plain), arr, n.value, byref(n))
+        return [(r.group, r.sum, r.count) for r in arr[:n.value]]
+
+    def stats(self) -> BatchStats:
+        st = BatchStats()
+        _call("mgv_batch_stats_get", self.h, byref(st))
+        return st
+
+    def destroy(self) -> None:
+        if self.h:
+            load().mgv_batch_destroy(self.h)
+            self.h = None
+
+
+def batch_autotune(ctx: Context, queries) -> BatchConfig:
+    arr = (QueryDesc * max(1, len(queries)))(*queries)
+    cfg = BatchConfig()
+    _call("mgv_batch_autotune", ctx.h, arr, len(queries), byref(cfg))
+    return cfg
+
+
+class Server:
+    """mgv_server: continuous batching over resident build tables."""
+
+    def __init__(self, ctx: Context, memory_budget: int, max_batch: int = 0, max_inflight: int = 0,
+                 load_factor: float = 0.0, plain: bool = False):
+        h = c_void_p()
+        cfg = ServerConfig(memory_budget, max_batch, max_inflight, load_factor, int(plain))
+        _call("mgv_server_create", ctx.h, byref(cfg), byref(h))
+        self.h, self.ctx = h, ctx
+
+    def add_table(self, keys, rows: int, payloads=None) -> int:
+        t = c_uint32()
+        _call("mgv_server_add_table", self.h, c_void_p(_ptr(keys)),
+              None if payloads is None else c_void_p(_ptr(payloads)), rows, byref(t))
+        return t.value
+
+    def submit(self, table: int, key, filt, group, value, rows: int, bound: int, max_groups: int) -> int:
+        r = ServerRequest(table, 0, _ptr(key), _ptr(filt), _ptr(group), _ptr(value), rows, bound, max_groups)
+        t = c_uint64()
+        _call("mgv_server_submit", self.h, byref(r), byref(t))
+        return t.value
+
+    def try_submit(self, *args) -> tuple[int, int]:
+        table, key, filt, group, value, rows, bound, max_groups = args
+        r = ServerRequest(table, 0, _ptr(key), _ptr(filt), _ptr(group), _ptr(value), rows, bound, max_groups)
+        t = c_uint64()
+        st = load().mgv_server_submit(self.h, byref(r), byref(t))
+        return st, t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000, max_rows: int = 1 << 20):
+        arr = (GroupRow * max_rows)()
+        n = c_uint64()
+        lat = c_double()
+        st = load().mgv_server_wait(self.h, ticket, timeout_ms, arr, max_rows, byref(n), byref(lat))
+        return st, [(r.group, r.sum, r.count) for r in arr[:min(n.value, max_rows)]], lat.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _call("mgv_server_stats_get", self.h, byref(st))
+        return st
+
+    def reset_stats(self) -> None:
+        _call("mgv_server_reset_stats", self.h)
+
+    def destroy(self) -> None:
+        if self.h:
+            load().mgv_server_destroy(self.h)
             self.h = None
 
 
