@@ -195,6 +195,11 @@ def main():
     ap.add_argument("--rows-per-thread", type=int, default=None)
     ap.add_argument("--stages", type=int, default=None)
     ap.add_argument("--ctas-per-sm", type=int, default=None)
+    ap.add_argument("--workload", default="join", choices=["join", "select", "pipeline", "batched", "served"],
+                    help="join: the headline probe; the others are the remaining configurations")
+    ap.add_argument("--queries", type=int, default=512, help="batched: queries in the mix")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="served: arrival window per rate")
+    ap.add_argument("--rates", default="200,1000,5000", help="served: arrival rates (queries/s)")
     ap.add_argument("--gather-ceiling", action="store_true",
                     help="measure the random 32-byte bucket-read ceiling instead of the join")
     ap.add_argument("--settle-s", type=float, default=1.0, help="untimed steps before timing, in seconds")
@@ -207,6 +212,10 @@ def main():
     import torch
     import mgv
 
+    if args.workload != "join":
+        import workloads
+
+        return workloads.run(args)
     if args.gather_ceiling:
         ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
         out = []

@@ -1,0 +1,330 @@
+"""Benchmark workloads beside the headline join probe (run by bench.py --workload).
+
+  select    select + aggregate: 2^22 rows, c0 U[0,2^31) with c0 < 2^30, COUNT and
+            int64 SUM of c1 U[0,2^20); 8 B/row; the L2 is flushed between steps
+  pipeline  select -> join -> group-by: probe 2^27 rows (key over 2^24 build keys,
+            filter U[0,1000) <= 99, group Zipf(1) over 4096, value U[0,2^16)), build
+            2^24 keys radix-partitioned on 8 bits; 16 B/probe row + 4 B/build key
+  batched   512 select -> join -> group-by queries (build 2^U(10,22), probe
+            2^U(12,24), selectivity U(1%,90%), groups 2^U(4,16), join-style value
+            distributions) in one batch (CUDA graph replay) against the same queries
+            one at a time through the plain pipeline
+  served    open-loop Poisson arrivals of that mix at 200 / 1000 / 5000 queries/s
+            over 16 resident tables, 40 GB budget, continuous batching vs the plain
+            one-at-a-time server; p50 / p99 latency
+
+Every line is one JSON object; results are checked (batched against plain, the
+pipeline against the oracle on its known total) before anything is printed.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import statistics
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+HIT = 3865470566
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _line(args, metric, value, unit, ms, workload, extra, clk, higher=True):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": higher, "scaling": "weak",
+         "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": {"workload": workload}}
+    d.update(extra)
+    d["clocks"] = clk.summary()
+    print(json.dumps(d), flush=True)
+
+
+def run_select(args, mgv, torch, ctx, bench, clk):
+    n = 1 << 22
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        c0 = torch.empty(n, dtype=torch.int32, device="cuda")
+        c1 = torch.empty(n, dtype=torch.int32, device="cuda")
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ctx.gen_uniform(c0, n, 0x5EED0001, 0, 0, 1 << 31, stream=stream)
+    ctx.gen_uniform(c1, n, 0x5EED0001, 1, 0, 1 << 20, stream=stream)
+    head, agg = mgv.create_sum_select_pipeline(ctx, (1 << 30) - 1, 0, 1)
+    times = []
+    h0 = time.time()
+    for i in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)  # 256 MiB > L2: inputs come from HBM every step
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        head.open(stream)
+        head.consume_columns([c0, c1], n, stream)
+        head.close(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= args.warmup:
+            times.append(e0.elapsed_time(e1) / 1000.0)
+    clk.mark(h0, time.time())
+    cnt, s = agg.result()
+    t = statistics.median(times)
+    peak, kind = bench.measured_peaks()
+    _line(args, "select+aggregate rows/s", n / t, "rows/s", 1000 * t,
+          "select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between steps",
+          {"roofline": {"bound": "hbm", "achieved": 8 * n / t / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": 8 * n / t / 1e9 / peak, "peak_kind": kind},
+           "result": {"count": cnt, "sum": s},
+           "note": "step = open -> consume -> close incl. the host read-back; 33.5 MB per step"}, clk)
+    head.destroy()
+    agg.destroy()
+
+
+def run_pipeline(args, mgv, torch, ctx, bench, clk):
+    nb, npb = 1 << 24, 1 << 27
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+        cols = [torch.empty(npb, dtype=torch.int32, device="cuda") for _ in range(4)]
+    seed = 0x5EED0003
+    ctx.gen_perm(bk, nb, seed, stream=stream)
+    ctx.gen_uniform(cols[0], npb, seed, 1, 0, nb, stream=stream)
+    ctx.gen_uniform(cols[1], npb, seed, 2, 0, 1000, stream=stream)
+    ctx.gen_zipf(cols[2], npb, seed, 3, 4096, stream=stream)
+    ctx.gen_uniform(cols[3], npb, seed, 4, 0, 1 << 16, stream=stream)
+    qualifying = int((cols[1] <= 99).sum().item())
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8)
+    bt, pt = [], []
+    h0 = time.time()
+    for i in range(args.warmup + args.steps):
+        e0, e1, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        part.open(stream); part.consume_columns([bk], nb, stream); part.close(stream)
+        e1.record(stream)
+        sel.open(stream); sel.consume_columns(cols, npb, stream); sel.close(stream)
+        e2.record(stream)
+        stream.synchronize()
+        if i >= args.warmup:
+            bt.append(e0.elapsed_time(e1) / 1000.0)
+            pt.append(e1.elapsed_time(e2) / 1000.0)
+    clk.mark(h0, time.time())
+    res = gb.result()
+    total = sum(c for _, _, c in res)
+    assert total == qualifying, (total, qualifying)  # every probe key is a build key
+    b, p_ = statistics.median(bt), statistics.median(pt)
+    peak, kind = bench.measured_peaks()
+    alg = 16 * npb + 4 * nb
+    _line(args, "select->join->group-by probe rows/s", npb / (b + p_), "rows/s", 1000 * (b + p_),
+          "select (filter <= 99 of U[0,1000)) -> join (2^27 probe rows, key over 2^24 build keys) -> group-by "
+          "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key bits",
+          {"roofline": {"bound": "hbm", "achieved": alg / (b + p_) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / (b + p_) / 1e9 / peak, "peak_kind": kind,
+                        "algorithmic_bytes_per_step": alg},
+           "phases_ms": {"partition+build": 1000 * b, "select+probe+groupby": 1000 * p_},
+           "result": {"groups": len(res), "count": total}}, clk)
+    for o in (sel, gb, hb, part):
+        o.destroy()
+
+
+def _mix(ctx, torch, mgv, nq, seed, stream):
+    """The batched configuration: per query, build 2^U(10,22) unique keys,
+    probe 2^U(12,24) rows (key 90% from the build keys, filter U[0,1000),
+    group Zipf(1) over 2^U(4,16) groups, value U[0,2^20)), selectivity U(1%,90%)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    spec = []
+    for i in range(nq):
+        nb = int(2 ** rng.uniform(10, 22))
+        npr = int(2 ** rng.uniform(12, 24))
+        bound = int(round(rng.uniform(0.01, 0.90) * 1000)) - 1
+        g = int(2 ** rng.uniform(4, 16))
+        spec.append((nb, npr, bound, g))
+    tb, tp = sum(x[0] for x in spec), sum(x[1] for x in spec)
+    with torch.cuda.stream(stream):
+        B = torch.empty(tb, dtype=torch.int32, device="cuda")
+        P = [torch.empty(tp, dtype=torch.int32, device="cuda") for _ in range(4)]
+    descs = []
+    ob = op = 0
+    for i, (nb, npr, bound, g) in enumerate(spec):
+        s = seed * 100000 + i
+        bkey = B[ob:ob + nb]
+        pk, pf, pg, pv = [c[op:op + npr] for c in P]
+        ctx.gen_perm(bkey, nb, s, stream=stream)
+        ctx.gen_probe_keys(pk, npr, s + 1, s, nb, HIT, nb, (1 << 31) - nb, stream=stream)
+        ctx.gen_uniform(pf, npr, s + 1, 2, 0, 1000, stream=stream)
+        ctx.gen_zipf(pg, npr, s + 1, 3, g, stream=stream)
+        ctx.gen_uniform(pv, npr, s + 1, 4, 0, 1 << 20, stream=stream)
+        descs.append(mgv.query_desc(bkey, nb, pk, pf, pg, pv, npr, bound, g))
+        ob += nb
+        op += npr
+    stream.synchronize()
+    return spec, descs, (B, P)
+
+
+def run_batched(args, mgv, torch, ctx, bench, clk):
+    stream = torch.cuda.Stream()
+    nq = args.queries
+    spec, descs, keep = _mix(ctx, torch, mgv, nq, 0x5EED0004, stream)
+    t0 = time.perf_counter()
+    cfg = mgv.batch_autotune(ctx, descs)
+    tune_s = time.perf_counter() - t0
+    b = mgv.Batch(ctx, descs, cfg, keep)
+    bt, pt = [], []
+    h0 = time.time()
+    for i in range(args.warmup + args.steps):
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        b.run(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= args.warmup:
+            bt.append(e0.elapsed_time(e1) / 1000.0)
+    clk.mark(h0, time.time())
+    plain_steps = max(1, min(args.steps, 3))
+    for i in range(1 + plain_steps):
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        b.run_plain(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= 1:
+            pt.append(e0.elapsed_time(e1) / 1000.0)
+    mism = sum(1 for q in range(nq) if b.result(q) != b.result(q, plain=True))
+    assert mism == 0, f"{mism} queries differ between batched and plain"
+    tb, tp = statistics.median(bt), statistics.median(pt)
+    rows = sum(x[1] for x in spec)
+    st = b.stats()
+    _line(args, "batched queries/s vs plain", nq / tb, "queries/s", 1000 * tb,
+          f"{nq} select->join->group-by queries, build 2^U(10,22), probe 2^U(12,24) rows (total {rows}), "
+          "selectivity U(1%,90%), groups 2^U(4,16); one batch (CUDA graph replay) incl. results to host",
+          {"plain": {"value": nq / tp, "unit": "queries/s", "ms": 1000 * tp,
+                     "how": "the same queries one at a time: hash_build open/consume/close, then "
+                            "select->hash_probe->groupby open/consume/close, operators created once"},
+           "speedup_vs_plain": tp / tb,
+           "autotuned": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
+                         "probe_ctas_per_sm": cfg.probe_ctas_per_sm, "tune_s": tune_s},
+           "arena_bytes": st.arena_bytes, "probe_rows": rows,
+           "probe_rows_per_s": rows / tb, "checked": "all queries equal between batched and plain"}, clk)
+    b.destroy()
+
+
+def run_served(args, mgv, torch, ctx, bench, clk):
+    import numpy as np
+
+    stream = torch.cuda.Stream()
+    ntab = 16
+    rng = np.random.default_rng(0x5EED0005)
+    prows = 1 << 24
+    tables = []
+    for t in range(ntab):
+        nb = int(2 ** rng.uniform(10, 22))
+        g = int(2 ** rng.uniform(4, 16))
+        with torch.cuda.stream(stream):
+            bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+            cols = [torch.empty(prows, dtype=torch.int32, device="cuda") for _ in range(4)]
+        s = 0x5EED0005 * 100 + t
+        ctx.gen_perm(bk, nb, s, stream=stream)
+        ctx.gen_probe_keys(cols[0], prows, s + 1, s, nb, HIT, nb, (1 << 31) - nb, stream=stream)
+        ctx.gen_uniform(cols[1], prows, s + 1, 2, 0, 1000, stream=stream)
+        ctx.gen_zipf(cols[2], prows, s + 1, 3, g, stream=stream)
+        ctx.gen_uniform(cols[3], prows, s + 1, 4, 0, 1 << 20, stream=stream)
+        tables.append((nb, g, bk, cols))
+    stream.synchronize()
+    rates = [float(r) for r in args.rates.split(",")]
+
+    def trace(rate, seed):
+        r = np.random.default_rng(seed)
+        n = max(1, int(rate * args.serve_seconds))
+        gaps = r.exponential(1.0 / rate, n)
+        reqs = []
+        for i in range(n):
+            t = int(r.integers(ntab))
+            rows = int(2 ** r.uniform(12, 24))
+            bound = int(round(r.uniform(0.01, 0.90) * 1000)) - 1
+            reqs.append((t, rows, bound))
+        return np.cumsum(gaps), reqs
+
+    def serve(plain, rate, seed):
+        import ctypes
+        import hashlib
+        import queue
+        import threading
+
+        srv = mgv.Server(ctx, 40 << 30, max_batch=256, max_inflight=2, plain=plain)
+        tids = [srv.add_table(bk, nb) for nb, g, bk, cols in tables]
+        for i, (nb, g, bk, cols) in enumerate(tables):  # warm-up: one request per table
+            st, _, _ = srv.wait(srv.submit(tids[i], *cols, 4096, 500, g), 600000, 1 << 16)
+            assert st == mgv.OK
+        srv.reset_stats()
+        at, reqs = trace(rate, seed)
+        # Results are drained by a second thread while requests arrive (the
+        # ctypes wait releases the GIL); each is kept as a digest of its rows.
+        tq: "queue.Queue[int | None]" = queue.Queue()
+        digests, errs = [], []
+
+        def drain():
+            buf = (mgv.GroupRow * (1 << 16))()
+            n, lat = ctypes.c_uint64(), ctypes.c_double()
+            while True:
+                tk = tq.get()
+                if tk is None:
+                    return
+                st = mgv.load().mgv_server_wait(srv.h, tk, 600000, buf, 1 << 16, ctypes.byref(n), ctypes.byref(lat))
+                if st != mgv.OK:
+                    errs.append(st)
+                digests.append(hashlib.blake2b(memoryview(buf).cast("B")[:n.value * ctypes.sizeof(mgv.GroupRow)],
+                                               digest_size=16).digest())
+
+        th = threading.Thread(target=drain)
+        th.start()
+        t0 = time.perf_counter()
+        for a, (t, rows, bound) in zip(at, reqs):
+            while time.perf_counter() - t0 < a:
+                pass
+            nb, g, bk, cols = tables[t]
+            tq.put(srv.submit(tids[t], *cols, rows, bound, g))
+        t_sub = time.perf_counter() - t0
+        tq.put(None)
+        th.join()
+        wall = time.perf_counter() - t0
+        assert not errs, errs
+        stats = srv.stats()
+        srv.destroy()
+        return {"offered_qps": rate, "arrived_qps": len(reqs) / t_sub, "requests": len(reqs),
+                "throughput_qps": len(reqs) / wall, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
+                "mean_ms": stats.mean_ms, "max_ms": stats.max_ms, "batches": stats.batches,
+                "mean_batch": stats.mean_batch, "peak_device_bytes": stats.peak_bytes}, digests
+
+    out = []
+    h0 = time.time()
+    for k, rate in enumerate(rates):
+        b, rb = serve(False, rate, 1000 + k)
+        p, rp = serve(True, rate, 1000 + k)
+        assert rb == rp, "served results differ from the plain server"
+        out.append({"rate": rate, "batched": b, "plain": p})
+    clk.mark(h0, time.time())
+    best = out[-1]
+    _line(args, "served queries/s & p99 latency vs plain", best["batched"]["throughput_qps"], "queries/s",
+          best["batched"]["mean_ms"],
+          "open-loop Poisson arrivals of the batched mix over 16 resident tables (build 2^U(10,22), probe "
+          "2^U(12,24) rows, selectivity U(1%,90%), groups 2^U(4,16)); 40 GB budget; continuous batching",
+          {"rates": out, "checked": "every request's result equals the plain server's"}, clk)
+
+
+def run(args) -> int:
+    sys.path.insert(0, HERE)
+    import torch
+
+    import bench  # the repo-root benchmark script: peaks and clock sampling
+    import mgv
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    fn = {"select": run_select, "pipeline": run_pipeline, "batched": run_batched, "served": run_served}[args.workload]
+    with bench.ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        fn(args, mgv, torch, ctx, bench, clk)
+    ctx.close()
+    return 0
