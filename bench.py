@@ -198,6 +198,8 @@ def main():
     ap.add_argument("--workload", default="join", choices=["join", "select", "pipeline", "batched", "served"],
                     help="join: the headline probe; the others are the remaining configurations")
     ap.add_argument("--queries", type=int, default=512, help="batched: queries in the mix")
+    ap.add_argument("--batch-config", default=None,
+                    help="batched: 'load_factor,probe_item_rows,item_order' instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--rates", default="200,1000,5000", help="served: arrival rates (queries/s)")
     ap.add_argument("--gather-ceiling", action="store_true",

@@ -90,7 +90,8 @@ typedef struct mgv_tuning {
     uint32_t probe_ctas_per_sm;     /* 0 = as many as fit; 3 with 4 rows per thread
                                        selects the 3-CTA register budget               */
     float default_load_factor;      /* hash_build tables whose desc gives 0            */
-    uint32_t groupby_smem_slots;    /* per-CTA shared group table (power of 2, 0 = off) */
+    uint32_t groupby_smem_slots;    /* largest per-CTA shared group table: 0 (off) or a
+                                       power of 2 in [64, 8192]; default 8192        */
     uint32_t reserved[2];
 } mgv_tuning;
 
@@ -342,7 +343,11 @@ typedef struct mgv_batch_config {
     uint32_t probe_item_rows;   /* rows per probe work item (0 = 32768)         */
     uint32_t probe_ctas_per_sm; /* 0 = as many as fit                           */
     uint32_t use_graph;         /* 1 = capture once, replay as a CUDA graph     */
-    uint32_t reserved[3];
+    uint32_t item_order;        /* 0 = work items dealt round-robin to the CTAs
+                                   (all CTAs on neighbouring items, so the
+                                   tables in use stay in L2); 1 = one
+                                   contiguous run of items per CTA             */
+    uint32_t reserved[2];
 } mgv_batch_config;
 
 typedef struct mgv_batch mgv_batch;

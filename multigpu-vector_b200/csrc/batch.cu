@@ -103,7 +103,8 @@ mgv_status enqueue_run(mgv_batch* b, cudaStream_t s) {
     MGV_CUDA_TRY(cudaMemsetAsync(b->group_zero, 0, b->group_zero_bytes, s));
     MGV_CUDA_TRY(cudaMemsetAsync(b->out_counts, 0, sizeof(uint32_t) * b->q.size(), s));
     MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_builds, b->d_outs, b->d_build_items, b->n_build, b->d_probe_items,
-                              b->n_probe, b->d_compact_items, b->n_compact, (int)b->cfg.probe_ctas_per_sm, s, ctx));
+                              b->n_probe, b->d_compact_items, b->n_compact, (int)b->cfg.probe_ctas_per_sm,
+                              b->cfg.item_order, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->out_counts, sizeof(uint32_t) * b->q.size(), cudaMemcpyDeviceToHost, s));
     if (b->out_rows_total)
         MGV_CUDA_TRY(cudaMemcpyAsync(b->h_rows, b->out_rows, sizeof(mgv_group_row) * b->out_rows_total,
@@ -143,6 +144,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     if (cfg.build_item_rows == 0) cfg.build_item_rows = 65536;
     if (cfg.probe_item_rows == 0) cfg.probe_item_rows = 32768;
     if (cfg.probe_item_rows % 128) return fail(MGV_EINVAL, "probe_item_rows must be a multiple of 128");
+    if (cfg.item_order > 1) return fail(MGV_EINVAL, "item_order must be 0 or 1");
     for (uint32_t i = 0; i < nq; ++i) {
         const mgv_query_desc& d = qs[i];
         if ((d.build_rows && !d.build_keys) ||
@@ -281,7 +283,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         c.ref[1] = 2;  // value
         c.nref = 2;
         c.gt = g;
-        c.smem_groups = gcap[i] <= 4096 ? 1u : 0u;
+        c.smem_groups = std::min(gcap[i], kMaxSmemGroups);
         hb[i] = BatchBuild{qs[i].build_keys, qs[i].build_payloads, t};
         ho[i] = BatchOut{g, b->out_rows + b->out_offset[i], b->out_counts + i, qs[i].max_groups, 0};
     }
@@ -429,18 +431,19 @@ mgv_status mgv_batch_autotune(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t n
     if (!ctx || (!qs && nq) || !out) return fail(MGV_EINVAL, "NULL argument");
     const float lfs[] = {0.4f, 0.5f, 0.6f};
     const uint32_t items[] = {8192, 32768, 131072};
-    const uint32_t ctas[] = {0, 1};
+    const uint32_t orders[] = {0, 1};
     double best = 1e30;
     mgv_batch_config best_cfg{};
     for (float lf : lfs)
         for (uint32_t it : items)
-            for (uint32_t c : ctas) {
+            for (uint32_t order : orders) {
                 mgv_batch_config cfg{};
                 cfg.load_factor = lf;
                 cfg.build_item_rows = 65536;
                 cfg.probe_item_rows = it;
-                cfg.probe_ctas_per_sm = c;
+                cfg.probe_ctas_per_sm = 0;
                 cfg.use_graph = 1;
+                cfg.item_order = order;
                 mgv_batch* b = nullptr;
                 mgv_status st = mgv_batch_create(ctx, qs, nq, &cfg, &b);
                 if (st != MGV_OK) return st;

@@ -142,7 +142,9 @@ mgv_status mgv_ctx_info_get(mgv_ctx* ctx, mgv_ctx_info* out) {
     out->hbm_bytes = (uint64_t)ctx->prop.totalGlobalMem;
     out->cc_major = ctx->prop.major;
     out->cc_minor = ctx->prop.minor;
-    std::snprintf(out->name, sizeof(out->name), "%s", ctx->prop.name);
+    const size_t len = strnlen(ctx->prop.name, sizeof(out->name) - 1);  // truncated to the field
+    std::memcpy(out->name, ctx->prop.name, len);
+    out->name[len] = '\0';
     return MGV_OK;
 }
 
@@ -164,6 +166,9 @@ mgv_status mgv_ctx_set_tuning(mgv_ctx* ctx, const mgv_tuning* t) {
     if (t->probe_ctas_per_sm > 32) return fail(MGV_EINVAL, "probe_ctas_per_sm out of range");
     if (!(t->default_load_factor > 0.0f && t->default_load_factor <= 0.95f))
         return fail(MGV_EINVAL, "default_load_factor must be in (0, 0.95]");
+    const uint32_t gs = t->groupby_smem_slots;
+    if (gs != 0 && (gs < 64 || gs > kMaxSmemGroups || (gs & (gs - 1)) != 0))
+        return fail(MGV_EINVAL, "groupby_smem_slots must be 0 or a power of two in [64, 8192]");
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuning = *t;
     return MGV_OK;

@@ -30,9 +30,12 @@
 
 namespace mgv {
 
-constexpr int kChainBlock = 256;
+constexpr int kChainBlock = 512;  // 16 warps: one CTA per SM with the largest group table
 constexpr int kChainWarps = kChainBlock / 32;
-constexpr int kRing = 256;
+constexpr int kWinRows = 512;  // rows per warp per select window: 16 loads per lane in flight
+constexpr int kIdRing = 1024;  // per-warp ring of qualifying row offsets (>= kWinRows + 127)
+constexpr int kMaxTermSlots = 3;  // carried columns of an aggregate / group-by chain: key + 2 references
+constexpr size_t kRingBytes = (size_t)kChainWarps * kIdRing * sizeof(uint32_t);
 
 
 // ---- device buffer pool: pop (swap-on-full for the sink) -------------------
@@ -124,7 +127,17 @@ __device__ __forceinline__ void sink_emit_warp(const SinkView& s, uint32_t my_cn
 }
 
 // ---- group tables ------------------------------------------------------------
+//
+// Both tables use Fibonacci hashing, (g * 2654435769) >> (32 - log2 cap), and
+// linear probing; a slot's key goes from EMPTY (INT32_MIN) to its group once
+// (atomicCAS) and never changes until the table is cleared, so a reader that
+// sees a stale EMPTY just loses the CAS and reads the winner's key.
 
+__device__ __forceinline__ uint32_t group_hash(int32_t g, uint32_t cap) {
+    return ((uint32_t)g * 2654435769u) >> (__clz(cap) + 1);  // cap = 2^k: shift = 32 - k
+}
+
+// Adds (sum, cnt) to group g of the global table; the adds are fire-and-forget.
 __device__ __forceinline__ void global_group_add(const GroupTableView& gt, int32_t g, unsigned long long sum,
                                                  unsigned long long cnt, uint32_t* err) {
     if (g == kEmptyKey) {  // the reserved key has its own counters
@@ -132,9 +145,9 @@ __device__ __forceinline__ void global_group_add(const GroupTableView& gt, int32
         atomicAdd(gt.special + 1, cnt);
         return;
     }
-    uint32_t slot = murmur32((uint32_t)g) & (gt.cap - 1);
+    uint32_t slot = group_hash(g, gt.cap);
     for (uint32_t i = 0; i < gt.cap; ++i) {
-        int32_t k = *((volatile int32_t*)(gt.keys + slot));
+        int32_t k = gt.keys[slot];
         if (k == kEmptyKey) k = atomicCAS(gt.keys + slot, kEmptyKey, g);
         if (k == kEmptyKey || k == g) {
             atomicAdd(gt.sums + slot, sum);
@@ -146,107 +159,169 @@ __device__ __forceinline__ void global_group_add(const GroupTableView& gt, int32
     set_error(err, kDevTableFull, 20);
 }
 
+// A CTA's shared group table: cap slots plus one for the reserved group
+// INT32_MIN, all 32-bit so that every update is a native shared atomic.
+// The int64 sum of a slot is kept biased, as sum + count * 2^31 in two words
+// (lo, hi): a value v adds v + 2^31, which lies in [0, 2^32), to lo and a
+// carry to hi.
 struct SmemGroups {
     int32_t* keys;
-    unsigned long long* sums;
-    uint32_t* counts;
-    uint32_t cap;  // 0 = no shared table
+    uint32_t* cnt;
+    uint32_t* lo;
+    uint32_t* hi;
+    uint32_t cap;  // power of two, 0 = no shared table
 };
 
-__device__ __forceinline__ void group_insert(const SmemGroups& sg, const GroupTableView& gt, int32_t g, long long sum,
-                                             uint32_t cnt, uint32_t* err) {
-    if (sg.cap && g != kEmptyKey) {
-        uint32_t slot = murmur32((uint32_t)g) & (sg.cap - 1);
-#pragma unroll 1
-        for (int i = 0; i < 8; ++i) {
-            int32_t k = sg.keys[slot];
-            if (k == kEmptyKey) k = atomicCAS(sg.keys + slot, kEmptyKey, g);
-            if (k == kEmptyKey || k == g) {
-                atomicAdd(sg.sums + slot, (unsigned long long)sum);
-                atomicAdd(sg.counts + slot, cnt);
-                return;
-            }
-            slot = (slot + 1) & (sg.cap - 1);
-        }
-    }
-    global_group_add(gt, g, (unsigned long long)sum, cnt, err);
+constexpr uint32_t kGroupProbes = 16;  // shared-table probes before a row goes to the global table
+
+__host__ __device__ __forceinline__ size_t smem_groups_bytes(uint32_t cap) { return cap ? (size_t)(cap + 1) * 16 : 0; }
+
+__device__ __forceinline__ SmemGroups smem_groups_at(unsigned char* base, uint32_t cap) {
+    SmemGroups sg;
+    sg.keys = reinterpret_cast<int32_t*>(base);
+    sg.cnt = reinterpret_cast<uint32_t*>(base) + (cap + 1);
+    sg.lo = reinterpret_cast<uint32_t*>(base) + 2 * (cap + 1);
+    sg.hi = reinterpret_cast<uint32_t*>(base) + 3 * (cap + 1);
+    sg.cap = cap;
+    return sg;
 }
 
-// Warp-collective: add (g, v) for every active lane.  Lanes with the same
-// group are combined first; the sum of up to 32 int32 values is exact from
-// two 16-bit halves (each half-sum stays below 2^21).
-__device__ __forceinline__ void group_add_warp(bool active, int32_t g, int32_t v, const SmemGroups& sg,
-                                               const GroupTableView& gt, uint32_t* err) {
-    const unsigned act = __ballot_sync(0xffffffffu, active);
-    if (!act || !active) return;
-    const unsigned peers = __match_any_sync(act, g);
-    const uint32_t lo = (uint32_t)v & 0xffffu;
-    const uint32_t hi = (uint32_t)((v >> 16) + 32768);
-    const uint32_t slo = __reduce_add_sync(peers, lo);
-    const uint32_t shi = __reduce_add_sync(peers, hi);
-    if ((int)lane_id() == __ffs(peers) - 1) {
-        const uint32_t c = __popc(peers);
-        const long long sum = ((long long)shi - 32768ll * c) * 65536ll + (long long)slo;
-        group_insert(sg, gt, g, sum, c, err);
+// One row (g, v) of a group-by, per lane.
+__device__ __forceinline__ void group_add_row(const SmemGroups& sg, const GroupTableView& gt, int32_t g, int32_t v,
+                                              uint32_t* err) {
+    if (sg.cap) {
+        uint32_t slot = sg.cap;  // the reserved group's slot
+        bool hit = g == kEmptyKey;
+        if (!hit) {
+            slot = group_hash(g, sg.cap);
+#pragma unroll 1
+            for (uint32_t i = 0; i < kGroupProbes; ++i) {
+                int32_t k = *((volatile int32_t*)(sg.keys + slot));
+                if (k == kEmptyKey) k = atomicCAS(sg.keys + slot, kEmptyKey, g);
+                if (k == kEmptyKey || k == g) {
+                    hit = true;
+                    break;
+                }
+                slot = (slot + 1) & (sg.cap - 1);
+            }
+        }
+        if (hit) {
+            const uint32_t x = (uint32_t)v ^ 0x80000000u;  // v + 2^31
+            atomicAdd(sg.cnt + slot, 1u);
+            const uint32_t old = atomicAdd(sg.lo + slot, x);
+            if (old + x < old) atomicAdd(sg.hi + slot, 1u);
+            return;
+        }
+    }
+    global_group_add(gt, g, (unsigned long long)(long long)v, 1ull, err);
+}
+
+__device__ __forceinline__ void smem_groups_init(const SmemGroups& sg) {
+    for (uint32_t i = threadIdx.x; i <= sg.cap; i += blockDim.x) {
+        sg.keys[i] = kEmptyKey;
+        sg.cnt[i] = 0;
+        sg.lo[i] = 0;
+        sg.hi[i] = 0;
+    }
+}
+
+__device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const GroupTableView& gt, uint32_t* err) {
+    for (uint32_t i = threadIdx.x; i <= sg.cap; i += blockDim.x) {
+        const uint32_t c = sg.cnt[i];
+        if (c == 0) continue;
+        const unsigned long long biased = ((unsigned long long)sg.hi[i] << 32) | sg.lo[i];
+        const unsigned long long sum = biased - ((unsigned long long)c << 31);
+        global_group_add(gt, i == sg.cap ? kEmptyKey : sg.keys[i], sum, c, err);
     }
 }
 
 // ---- the chain: per-warp processing of a row range ------------------------------
 
-// Windows of 128 rows of [row_lo, row_hi), this warp taking windows
-// win_first, win_first + win_stride, ...: select into the warp's ring,
-// push full vectors through the probe and the terminal, flush the last
-// partial vector.
+// Value of carried slot `slot` (a run-time index) from the registers of a
+// vector; j is a compile-time row position after unrolling.
+template <int NS>
+__device__ __forceinline__ int32_t pick_slot(const int32_t (&v)[NS][4], int32_t slot, int j) {
+    int32_t r = 0;
+#pragma unroll
+    for (int c = 0; c < NS; ++c)
+        if (slot == c) r = v[c][j];
+    return r;
+}
+
+// Windows of kWinRows rows of [row_lo, row_hi) (fewer than 2^32 rows), this
+// warp taking windows win_first, win_first + win_stride, ...
+//
+// A window is filtered with 16 independent coalesced loads per lane (one
+// 128-byte warp load each, all in flight together), and the offsets of its
+// qualifying rows are compacted with __ballot_sync / __popc into the warp's
+// shared ring, in row order.  Every 128 offsets form a vector: its carried
+// columns are gathered into registers (4 rows per lane, all loads
+// independent), its keys probed, and its rows handed to the terminal.  Only
+// qualifying rows' columns are ever loaded.
 template <bool SEL, bool PROBE, int TERM>
 __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, uint64_t row_lo, uint64_t row_hi,
-                                              uint64_t win_first, uint64_t win_stride, int32_t* ring,
+                                              uint64_t win_first, uint64_t win_stride, uint32_t* ids,
                                               const SmemGroups& sg, unsigned long long& acnt,
                                               unsigned long long& asum, uint32_t* err) {
+    constexpr int NS = TERM == kTermSink ? MGV_MAX_COLS : kMaxTermSlots;
     const uint32_t lane = lane_id();
-    // value of terminal reference r for ring row rp and build payload bp
-    auto val = [&](int32_t ref, uint32_t rp, int32_t bp) -> int32_t {
-        return ref == kBP ? bp : ring[ref * kRing + rp];
-    };
-    // one output row (warp-collective)
-    auto emit = [&](bool active, uint32_t rp, int32_t bp) {
-        if (TERM == kTermAgg) {
-            if (active) {
-                long long t = 0;
-                if (a.ref[0] >= 0) t += val(a.ref[0], rp, bp);
-                if (a.ref[1] >= 0) t += val(a.ref[1], rp, bp);
-                acnt += 1;
-                asum += (unsigned long long)t;
-            }
-        } else if (TERM == kTermGroupby) {
-            const int32_t g = active ? val(a.ref[0], rp, bp) : 0;
-            const int32_t v = (active && a.ref[1] >= 0) ? val(a.ref[1], rp, bp) : 0;
-            group_add_warp(active, g, v, sg, a.gt, err);
-        } else {
-            sink_emit_warp(
-                a.sink, active ? 1u : 0u, [&](uint32_t, uint32_t col) { return val(a.ref[col], rp, bp); }, err);
-        }
-    };
+    const uint32_t len = (uint32_t)(row_hi - row_lo);
 
-    // push `cnt` (<= 128) dense ring rows starting at `start`
+    // push `cnt` (<= 128) offsets of the ring starting at `start`
     auto push_vector = [&](uint32_t start, uint32_t cnt) {
         __syncwarp();
-        if (!PROBE) {
-#pragma unroll 1
-            for (int j = 0; j < 4; ++j) {
-                const uint32_t idx = j * 32 + lane;
-                emit(idx < cnt, (start + idx) & (kRing - 1), 0);
+        uint32_t rid[4];
+        bool in[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t idx = j * 32 + lane;
+            in[j] = idx < cnt;
+            rid[j] = ids[(start + idx) & (kIdRing - 1)];
+        }
+        int32_t v[NS][4];
+#pragma unroll
+        for (int c = 0; c < NS; ++c) {
+            const bool carried = (uint32_t)c < a.nslots;
+            const int32_t* col = carried ? a.cols[a.slot_src[c]] + row_lo : nullptr;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[c][j] = (carried && in[j]) ? __ldg(col + rid[j]) : 0;
+        }
+        // value of terminal reference r for the lane's row j and build payload bp
+        auto val = [&](int32_t ref, int j, int32_t bp) -> int32_t {
+            return ref == kBP ? bp : pick_slot<NS>(v, ref, j);
+        };
+        // one output row (warp-collective)
+        auto emit = [&](bool active, int j, int32_t bp) {
+            if (TERM == kTermAgg) {
+                if (active) {
+                    long long t = 0;
+                    if (a.ref[0] >= 0) t += val(a.ref[0], j, bp);
+                    if (a.ref[1] >= 0) t += val(a.ref[1], j, bp);
+                    acnt += 1;
+                    asum += (unsigned long long)t;
+                }
+            } else if (TERM == kTermGroupby) {
+                if (active) {
+                    const int32_t g = val(a.ref[0], j, bp);
+                    const int32_t x = a.ref[1] >= 0 ? val(a.ref[1], j, bp) : 0;
+                    group_add_row(sg, a.gt, g, x, err);
+                }
+            } else {
+                sink_emit_warp(
+                    a.sink, active ? 1u : 0u, [&](uint32_t, uint32_t col) { return val(a.ref[col], j, bp); }, err);
             }
+        };
+        if (!PROBE) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) emit(in[j], j, 0);
         } else {
             // home-bucket loads of all four rows first, then walk each run
             uint32_t w[4][8];
             uint32_t hb[4];
             int32_t key[4];
-            bool in[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const uint32_t idx = j * 32 + lane;
-                in[j] = idx < cnt;
-                key[j] = in[j] ? ring[a.probe_slot * kRing + ((start + idx) & (kRing - 1))] : 0;
+                key[j] = pick_slot<NS>(v, a.probe_slot, j);
                 hb[j] = home_bucket(key[j], a.table);
                 if (in[j] && key[j] != kEmptyKey) ld_bucket(a.table.slots + 4ull * hb[j], w[j]);
             }
@@ -254,7 +329,6 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                 (uint32_t)min((unsigned long long)a.table.meta[0], (unsigned long long)a.table.side_cap);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const uint32_t rp = (start + j * 32 + lane) & (kRing - 1);
                 uint32_t wb[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) wb[q] = w[j][q];
@@ -292,69 +366,59 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                             done = true;
                         }
                     }
-                    emit(found, rp, bp);
+                    emit(found, j, bp);
                 }
             }
         }
         __syncwarp();
     };
 
-    const uint64_t nwin = (row_hi - row_lo + 127) / 128;
-    uint32_t head = 0, fill = 0;
+    const int32_t* __restrict__ fcol = SEL ? a.cols[a.sel_col] + row_lo : nullptr;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint64_t nwin = (len + kWinRows - 1) / kWinRows;
+    uint32_t head = 0, fill = 0;  // fill < 128 between windows
     for (uint64_t win = win_first; win < nwin; win += win_stride) {
-        const uint64_t r0 = row_lo + win * 128;
-#pragma unroll 1
-        for (int j = 0; j < 4; ++j) {
-            const uint64_t row = r0 + j * 32 + lane;
-            bool pass = row < row_hi;
-            if (SEL && pass) pass = __ldg(a.cols[a.sel_col] + row) <= a.sel_bound;
+        const uint32_t r0 = (uint32_t)win * kWinRows;
+        int32_t f[kWinRows / 32];
+        if (SEL) {
+#pragma unroll
+            for (int k = 0; k < kWinRows / 32; ++k) {
+                const uint32_t row = r0 + k * 32 + lane;
+                f[k] = row < len ? __ldg(fcol + row) : 0;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kWinRows / 32; ++k) {
+            const uint32_t row = r0 + k * 32 + lane;
+            const bool pass = row < len && (!SEL || f[k] <= a.sel_bound);
             const unsigned m = __ballot_sync(0xffffffffu, pass);
-            if (pass) {
-                const uint32_t pos = (head + fill + __popc(m & ((1u << lane) - 1u))) & (kRing - 1);
-                for (uint32_t c = 0; c < a.nslots; ++c) ring[c * kRing + pos] = __ldg(a.cols[a.slot_src[c]] + row);
-            }
+            if (pass) ids[(head + fill + __popc(m & lt)) & (kIdRing - 1)] = row;
             fill += __popc(m);
-            if (fill >= 128) {
-                push_vector(head, 128);
-                head = (head + 128) & (kRing - 1);
-                fill -= 128;
-            }
+        }
+        while (fill >= 128) {
+            push_vector(head, 128);
+            head = (head + 128) & (kIdRing - 1);
+            fill -= 128;
         }
     }
     if (fill) push_vector(head, fill);
 }
 
-__device__ __forceinline__ void smem_groups_init(const SmemGroups& sg) {
-    for (uint32_t i = threadIdx.x; i < sg.cap; i += blockDim.x) {
-        sg.keys[i] = kEmptyKey;
-        sg.sums[i] = 0;
-        sg.counts[i] = 0;
-    }
-}
-
-__device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const GroupTableView& gt, uint32_t* err) {
-    for (uint32_t i = threadIdx.x; i < sg.cap; i += blockDim.x)
-        if (sg.keys[i] != kEmptyKey && sg.counts[i]) global_group_add(gt, sg.keys[i], sg.sums[i], sg.counts[i], err);
-}
-
 template <bool SEL, bool PROBE, int TERM>
-__global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err) {
+__global__ void __launch_bounds__(kChainBlock, 1) k_chain(ChainDev a, uint32_t* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t warp = threadIdx.x / 32;
-    // shared layout: [group sums u64 | rings int32 | group keys int32 | group counts u32]
-    SmemGroups sg{nullptr, nullptr, nullptr, 0};
-    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + (TERM == kTermGroupby ? a.smem_groups * 8 : 0));
+    // shared layout: [id rings | group table]
+    uint32_t* rings = reinterpret_cast<uint32_t*>(smem_raw);
+    SmemGroups sg{nullptr, nullptr, nullptr, nullptr, 0};
     if (TERM == kTermGroupby && a.smem_groups) {
-        sg.sums = reinterpret_cast<unsigned long long*>(smem_raw);
-        sg.keys = rings + kChainWarps * a.nslots * kRing;
-        sg.counts = reinterpret_cast<uint32_t*>(sg.keys + a.smem_groups);
-        sg.cap = a.smem_groups;
+        sg = smem_groups_at(smem_raw + kRingBytes, a.smem_groups);
         smem_groups_init(sg);
         __syncthreads();
     }
     unsigned long long acnt = 0, asum = 0;
     chain_windows<SEL, PROBE, TERM>(a, a.unique != 0, 0, a.n, (uint64_t)blockIdx.x * kChainWarps + warp,
-                                    (uint64_t)gridDim.x * kChainWarps, rings + (size_t)warp * a.nslots * kRing, sg,
+                                    (uint64_t)gridDim.x * kChainWarps, rings + (size_t)warp * kIdRing, sg,
                                     acnt, asum, err);
     if (TERM == kTermAgg) block_accumulate2<kChainBlock>(acnt, asum, a.acc);
     if (TERM == kTermGroupby && a.smem_groups) {
@@ -365,74 +429,89 @@ __global__ void __launch_bounds__(kChainBlock) k_chain(ChainDev a, uint32_t* err
 
 // ---- batched queries ------------------------------------------------------------
 
-constexpr int kBatchSlots = 3;          // key, group, value
-constexpr uint32_t kBatchSmemGroups = 4096;
+// The work items of this CTA: item_order 0 deals them round-robin, so at any
+// moment all CTAs work on neighbouring items (in query order: the same few
+// queries, whose tables then stay in L2); 1 gives each CTA one contiguous run.
+struct ItemRange {
+    uint32_t first, end, step;
+};
+__device__ __forceinline__ ItemRange item_range(uint32_t nitems, uint32_t item_order) {
+    if (item_order == 0) return ItemRange{blockIdx.x, nitems, gridDim.x};
+    return ItemRange{(uint32_t)((uint64_t)blockIdx.x * nitems / gridDim.x),
+                     (uint32_t)((uint64_t)(blockIdx.x + 1) * nitems / gridDim.x), 1u};
+}
 
 // Probe phase of a batch: every CTA takes a contiguous run of (query, rows)
-// items in query order, so it stays on one query for many items; queries
-// with at most kBatchSmemGroups/2 groups aggregate in the CTA's shared table,
-// flushed to the query's global table when the CTA moves to another query.
-__global__ void __launch_bounds__(kChainBlock) k_batch_probe(const ChainDev* __restrict__ qs,
-                                                             const BatchItem* __restrict__ items, uint32_t nitems,
-                                                             uint32_t* err) {
+// items in query order, so it stays on one query for many items; each query
+// aggregates in the CTA's shared group table (up to kMaxSmemGroups slots;
+// rows whose group finds no shared slot go to the query's global table),
+// flushed to the global table when the CTA moves to another query.  The
+// current query's descriptor is copied to shared memory at each switch, so
+// its fields cost a shared load instead of registers or global loads.
+__global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* __restrict__ qs,
+                                                                const BatchItem* __restrict__ items,
+                                                                uint32_t nitems, uint32_t item_order, uint32_t* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ChainDev sq;
+    static_assert(sizeof(ChainDev) % 4 == 0, "ChainDev is copied as 32-bit words");
     const uint32_t warp = threadIdx.x / 32;
-    SmemGroups full_sg;
-    full_sg.sums = reinterpret_cast<unsigned long long*>(smem_raw);
-    int32_t* rings = reinterpret_cast<int32_t*>(smem_raw + kBatchSmemGroups * 8);
-    full_sg.keys = rings + kChainWarps * kBatchSlots * kRing;
-    full_sg.counts = reinterpret_cast<uint32_t*>(full_sg.keys + kBatchSmemGroups);
-    full_sg.cap = kBatchSmemGroups;
-    const SmemGroups no_sg{nullptr, nullptr, nullptr, 0};
+    uint32_t* rings = reinterpret_cast<uint32_t*>(smem_raw);
+    const SmemGroups no_sg{nullptr, nullptr, nullptr, nullptr, 0};
+    SmemGroups sg = no_sg;
 
-    const uint32_t it0 = (uint32_t)((uint64_t)blockIdx.x * nitems / gridDim.x);
-    const uint32_t it1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * nitems / gridDim.x);
+    const ItemRange r = item_range(nitems, item_order);
     int64_t cur = -1;
-    bool cur_smem = false;
     unsigned long long acnt = 0, asum = 0;
-    for (uint32_t it = it0; it < it1; ++it) {
+    for (uint32_t it = r.first; it < r.end; it += r.step) {
         const BatchItem item = items[it];
         if ((int64_t)item.q != cur) {
-            if (cur_smem) {
-                __syncthreads();
-                smem_groups_flush(full_sg, qs[cur].gt, err);
+            __syncthreads();  // every warp is done with the previous query
+            if (sg.cap) {
+                smem_groups_flush(sg, sq.gt, err);
+                __syncthreads();  // the flush is done reading sq and the shared table
             }
             cur = item.q;
-            cur_smem = qs[cur].smem_groups != 0;
-            if (cur_smem) {
-                __syncthreads();
-                smem_groups_init(full_sg);
-            }
+            for (uint32_t i = threadIdx.x; i < sizeof(ChainDev) / 4; i += kChainBlock)
+                reinterpret_cast<uint32_t*>(&sq)[i] = reinterpret_cast<const uint32_t*>(qs + cur)[i];
+            const uint32_t cap = qs[cur].smem_groups;
+            sg = cap ? smem_groups_at(smem_raw + kRingBytes, cap) : no_sg;
+            if (sg.cap) smem_groups_init(sg);
             __syncthreads();
         }
-        const ChainDev& a = qs[item.q];
+        const ChainDev& a = sq;
         const bool unique = a.table.meta[3] == 0;
         chain_windows<true, true, kTermGroupby>(a, unique, item.lo, item.hi, warp, kChainWarps,
-                                                rings + (size_t)warp * kBatchSlots * kRing,
-                                                cur_smem ? full_sg : no_sg, acnt, asum, err);
+                                                rings + (size_t)warp * kIdRing, sg, acnt, asum, err);
     }
-    if (cur_smem) {
+    if (sg.cap) {
         __syncthreads();
-        smem_groups_flush(full_sg, qs[cur].gt, err);
+        smem_groups_flush(sg, sq.gt, err);
     }
 }
 
 // Build phase of a batch: contiguous runs of (query, rows) items; every row
 // is inserted into its query's table.
-__global__ void __launch_bounds__(kChainBlock) k_batch_build(const BatchBuild* __restrict__ bs,
-                                                             const BatchItem* __restrict__ items, uint32_t nitems,
-                                                             uint32_t* err) {
-    const uint32_t it0 = (uint32_t)((uint64_t)blockIdx.x * nitems / gridDim.x);
-    const uint32_t it1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * nitems / gridDim.x);
-    for (uint32_t it = it0; it < it1; ++it) {
+__global__ void __launch_bounds__(kChainBlock, 2) k_batch_build(const BatchBuild* __restrict__ bs,
+                                                                const BatchItem* __restrict__ items, uint32_t nitems,
+                                                                uint32_t item_order, uint32_t* err) {
+    const ItemRange r = item_range(nitems, item_order);
+    for (uint32_t it = r.first; it < r.end; it += r.step) {
         const BatchItem item = items[it];
         const BatchBuild& b = bs[item.q];
+        constexpr int R = kBuildRows;
         bool dup = false;
         uint32_t inserted = 0;
-        for (uint64_t i = item.lo + threadIdx.x; i < item.hi; i += kChainBlock) {
-            bool ok;
-            table_insert(b.table, __ldg(b.keys + i), b.pays ? __ldg(b.pays + i) : 0, err, dup, ok);
-            inserted += ok;
+        for (uint64_t i0 = item.lo + threadIdx.x; i0 < item.hi; i0 += (uint64_t)kChainBlock * R) {
+            int32_t k[R], p[R];
+            bool valid[R];
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                const uint64_t i = i0 + (uint64_t)j * kChainBlock;
+                valid[j] = i < item.hi;
+                k[j] = valid[j] ? __ldg(b.keys + i) : 0;
+                p[j] = (valid[j] && b.pays) ? __ldg(b.pays + i) : 0;
+            }
+            table_insert_rows<R>(b.table, k, p, valid, err, dup, inserted);
         }
         const unsigned long long tot = warp_sum_u64(inserted);
         const unsigned any_dup = __any_sync(0xffffffffu, dup);
@@ -471,20 +550,20 @@ __global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchIt
 
 cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
                          const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
-                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, cudaStream_t s,
-                         Context* ctx) {
+                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
+                         cudaStream_t s, Context* ctx) {
     const int sms = ctx->prop.multiProcessorCount;
     if (n_build) {
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_build, kChainBlock, 0);
         const int grid = (int)std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, n_build);
-        k_batch_build<<<grid, kChainBlock, 0, s>>>(d_builds, build_items, n_build, ctx->d_err);
+        k_batch_build<<<grid, kChainBlock, 0, s>>>(d_builds, build_items, n_build, item_order, ctx->d_err);
         ctx->launches++;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (n_probe) {
-        const size_t smem = (size_t)kChainWarps * kBatchSlots * kRing * sizeof(int32_t) + (size_t)kBatchSmemGroups * 16;
+        const size_t smem = kRingBytes + smem_groups_bytes(kMaxSmemGroups);
         cudaError_t e = cudaFuncSetAttribute(k_batch_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         int per_sm = 0;
@@ -492,7 +571,7 @@ cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const
         per_sm = std::max(per_sm, 1);
         if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
         const int grid = (int)std::min<uint64_t>((uint64_t)per_sm * sms, n_probe);
-        k_batch_probe<<<grid, kChainBlock, smem, s>>>(d_qs, probe_items, n_probe, ctx->d_err);
+        k_batch_probe<<<grid, kChainBlock, smem, s>>>(d_qs, probe_items, n_probe, item_order, ctx->d_err);
         ctx->launches++;
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -513,12 +592,23 @@ static cudaError_t launch_chain_t(const ChainDev& d, size_t smem, uint64_t n, cu
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    int grid = occupancy_grid((const void*)k, kChainBlock, smem, ctx);
-    const uint64_t need = ((n + 127) / 128 + kChainWarps - 1) / kChainWarps;
-    if ((uint64_t)grid > need) grid = (int)(need ? need : 1);
-    k<<<grid, kChainBlock, smem, s>>>(d, ctx->d_err);
-    ctx->launches++;
-    return cudaGetLastError();
+    const int full = occupancy_grid((const void*)k, kChainBlock, smem, ctx);
+    // row offsets inside the kernel are 32-bit: launch at most 2^31 rows at a time
+    constexpr uint64_t kChunk = 1ull << 31;
+    for (uint64_t base = 0; base < n; base += kChunk) {
+        ChainDev c = d;
+        c.n = std::min<uint64_t>(kChunk, n - base);
+        for (uint32_t i = 0; i < c.ncols; ++i)
+            if (c.cols[i]) c.cols[i] += base;
+        int grid = full;
+        const uint64_t need = ((c.n + kWinRows - 1) / kWinRows + kChainWarps - 1) / kChainWarps;
+        if ((uint64_t)grid > need) grid = (int)(need ? need : 1);
+        k<<<grid, kChainBlock, smem, s>>>(c, ctx->d_err);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 template <int TERM>
@@ -558,9 +648,11 @@ cudaError_t launch_chain(const ChainArgs& a, cudaStream_t s, Context* ctx) {
     d.probe_slot = a.has_probe ? carry((int32_t)a.probe_col) : -1;
     d.nref = a.nref;
     for (uint32_t i = 0; i < a.nref; ++i) d.ref[i] = carry(a.ref[i]);
-    if (d.nslots == 0) d.slot_src[d.nslots++] = 0;  // keep one carried column for the ring
-    d.smem_groups = a.term == kTermGroupby ? a.smem_groups : 0;
-    const size_t smem = (size_t)kChainWarps * d.nslots * kRing * sizeof(int32_t) + (size_t)d.smem_groups * 16;
+    if (a.term != kTermSink && d.nslots > (uint32_t)kMaxTermSlots) return cudaErrorInvalidValue;
+    // the shared group table: as large as the global one (2 x max_groups, a
+    // power of two), capped by the tuning's slot limit
+    d.smem_groups = a.term == kTermGroupby ? std::min(a.smem_groups, a.gt.cap) : 0;
+    const size_t smem = kRingBytes + smem_groups_bytes(d.smem_groups);
     switch (a.term) {
         case kTermAgg: return launch_chain_term<kTermAgg>(a, d, smem, s, ctx);
         case kTermGroupby: return launch_chain_term<kTermGroupby>(a, d, smem, s, ctx);

@@ -55,6 +55,57 @@ __device__ __forceinline__ void table_insert(const TableView& t, int32_t key, in
     set_error(err, kDevTableFull, 2);
 }
 
+// Inserts R rows per thread with their latencies overlapped: the R home
+// buckets are loaded together, each row's first empty home slot is claimed
+// with one CAS (the R CASes in flight together), and only a row whose home
+// bucket is full or whose CAS lost a race takes the scalar path.  Any slot
+// read that already holds the row's key marks a duplicate (the row itself
+// is not in the table yet).
+template <int R>
+__device__ __forceinline__ void table_insert_rows(const TableView& t, const int32_t (&key)[R],
+                                                  const int32_t (&pay)[R], const bool (&valid)[R],
+                                                  uint32_t* err, bool& dup, uint32_t& inserted) {
+    unsigned long long s[R][4];
+    uint32_t b[R];
+    bool fast[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        fast[j] = valid[j] && key[j] != kEmptyKey;
+        b[j] = fast[j] ? home_bucket(key[j], t) : 0u;
+        if (fast[j]) ld_bucket_relaxed(t.slots + 4ull * b[j], s[j]);
+    }
+    int q[R];
+    unsigned long long v[R], old[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        q[j] = -1;
+        v[j] = ((unsigned long long)(uint32_t)pay[j] << 32) | (uint32_t)key[j];
+        if (!fast[j]) continue;
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            const int32_t sk = (int32_t)(uint32_t)s[j][k];
+            if (sk == kEmptyKey) q[j] = k;
+            if (sk == key[j]) dup = true;
+        }
+        // slots are claimed in order, so the first empty slot starts the free tail
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j)
+        old[j] = q[j] >= 0 ? atomicCAS(t.slots + 4ull * b[j] + q[j], kEmptySlot, v[j]) : 0ull;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        if (!valid[j]) continue;
+        if (q[j] >= 0 && old[j] == kEmptySlot) {
+            ++inserted;
+            continue;
+        }
+        if (q[j] >= 0 && (int32_t)(uint32_t)old[j] == key[j]) dup = true;
+        bool ok;
+        table_insert(t, key[j], pay[j], err, dup, ok);
+        inserted += ok;
+    }
+}
+
 // Matches of `key` inside one bucket w[0..7] = k0 p0 k1 p1 k2 p2 k3 p3.
 // more = the probe must continue to the next bucket.
 template <bool UNIQUE>

@@ -148,14 +148,21 @@ __global__ void __launch_bounds__(kBlock) k_build(const int32_t* __restrict__ ke
                                                   const int32_t* __restrict__ pays,
                                                   const int32_t* __restrict__ filt, int32_t bound,
                                                   uint64_t n, TableView t, uint32_t* err) {
+    constexpr int R = kBuildRows;
     bool dup = false;
     uint32_t inserted = 0;
-    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
-    for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n; i += stride) {
-        if (SEL && !(filt[i] <= bound)) continue;
-        bool ok;
-        table_insert(t, keys[i], pays ? pays[i] : 0, err, dup, ok);
-        inserted += ok;
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock * R;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * kBlock * R + threadIdx.x; i0 < n; i0 += stride) {
+        int32_t k[R], p[R];
+        bool valid[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const uint64_t i = i0 + (uint64_t)j * kBlock;
+            valid[j] = i < n && (!SEL || filt[i] <= bound);
+            k[j] = valid[j] ? keys[i] : 0;
+            p[j] = (valid[j] && pays) ? pays[i] : 0;
+        }
+        table_insert_rows<R>(t, k, p, valid, err, dup, inserted);
     }
     unsigned long long tot = warp_sum_u64(inserted);
     const unsigned any_dup = __any_sync(0xffffffffu, dup);
@@ -171,7 +178,7 @@ cudaError_t launch_build(const int32_t* keys, const int32_t* pays, const int32_t
     if (n == 0) return cudaSuccess;
     const void* k = has_sel ? (const void*)k_build<true> : (const void*)k_build<false>;
     int grid = occupancy_grid(k, kBlock, 0, ctx);
-    uint64_t need = (n + kBlock - 1) / kBlock;
+    uint64_t need = (n + (uint64_t)kBuildRows * kBlock - 1) / ((uint64_t)kBuildRows * kBlock);
     if ((uint64_t)grid > need) grid = (int)need;
     if (has_sel)
         k_build<true><<<grid, kBlock, 0, s>>>(keys, pays, filt, bound, n, t, ctx->d_err);

@@ -82,6 +82,11 @@ struct PoolDev {
 };
 
 constexpr uint32_t kNil = 0xffffffffu;
+#ifndef MGV_BUILD_ROWS_PER_THREAD
+#define MGV_BUILD_ROWS_PER_THREAD 1
+#endif
+constexpr int kBuildRows = MGV_BUILD_ROWS_PER_THREAD;  // build rows per thread in flight (1 measured fastest: more in flight contends in L2)
+constexpr uint32_t kMaxSmemGroups = 8192;  // largest per-CTA shared group table (slots; 128 KiB)
 
 // ---- host objects --------------------------------------------------------
 
@@ -110,7 +115,7 @@ struct Context {
     // pinned landing zone for close(): [0..1] error word, [2..] result words
     unsigned long long* h_stage = nullptr;
     std::atomic<uint64_t> launches{0};
-    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, 4096u, {0u, 0u}};
+    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, kMaxSmemGroups, {0u, 0u}};
     mgv_batch_config batch_tuned{};  // the batch autotuner's last choice
     bool has_batch_tuned = false;
     std::mutex mu;
@@ -229,7 +234,7 @@ struct ChainDev {
     uint32_t nref;
     unsigned long long* acc;
     GroupTableView gt;
-    uint32_t smem_groups;  // power of two, 0 = no shared table
+    uint32_t smem_groups;  // shared group-table slots: power of two <= kMaxSmemGroups, 0 = none
     SinkView sink;
 };
 
@@ -255,8 +260,8 @@ struct BatchOut {  // packed result region of a query
 };
 cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
                          const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
-                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, cudaStream_t s,
-                         Context* ctx);
+                         const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
+                         cudaStream_t s, Context* ctx);
 
 // partition.cu
 cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,

@@ -39,6 +39,7 @@ namespace {
 struct Request {
     uint64_t ticket = 0;
     mgv_server_request r{};
+    mgv_op* table = nullptr;  // the resident build table, resolved at submit
     Clock::time_point t_submit;
     double latency_ms = 0.0;
     mgv_status status = MGV_OK;
@@ -107,7 +108,8 @@ void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
     S->completed++;
 }
 
-// Launch one batch of admitted requests on slot `sl` (scheduler thread, lock held).
+// Launch one batch of admitted requests on slot `sl` (scheduler thread, lock
+// not held: it reads only the slot and its requests' immutable parameters).
 mgv_status launch(mgv_server* S, Inflight& sl) {
     Context* ctx = S->ctx;
     const uint32_t nq = (uint32_t)sl.reqs.size();
@@ -189,12 +191,12 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
         c.sel_col = 1;
         c.sel_bound = r.filter_bound;
         c.probe_slot = 0;
-        c.table = S->tables[r.table]->table;
+        c.table = sl.reqs[i]->table->table;
         c.ref[0] = 1;
         c.ref[1] = 2;
         c.nref = 2;
         c.gt = g;
-        c.smem_groups = caps[i] <= 4096 ? 1u : 0u;
+        c.smem_groups = std::min(caps[i], kMaxSmemGroups);
         ho[i] = BatchOut{g, reinterpret_cast<mgv_group_row*>(A + rows_off) + sl.offs[i],
                          reinterpret_cast<uint32_t*>(A + counts_off) + i, r.max_groups, 0};
     }
@@ -212,26 +214,31 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), nullptr,
                               reinterpret_cast<BatchOut*>(A + outs_off), nullptr, 0,
                               reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(),
-                              reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, s, ctx));
+                              reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, 0u, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
                                  cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaFreeAsync(sl.dmem, s));
     MGV_CUDA_TRY(cudaEventRecord(sl.done, s));
     sl.busy = true;
-    S->batches++;
-    S->batched_queries += nq;
     return MGV_OK;
 }
 
-// Results of a finished batch (lock held).
-void harvest(mgv_server* S, Inflight& sl) {
+// Copies a finished batch's rows out of the slot's pinned buffer into its
+// requests (scheduler thread, lock not held: nothing else touches the slot,
+// and waiters read a request's rows only after complete() under the lock).
+void collect(Inflight& sl) {
     for (size_t i = 0; i < sl.reqs.size(); ++i) {
         auto& q = sl.reqs[i];
         const uint32_t n = std::min<uint32_t>(sl.h_counts[i], q->r.max_groups);
         q->rows.assign(sl.h_rows + sl.offs[i], sl.h_rows + sl.offs[i] + n);
-        std::sort(q->rows.begin(), q->rows.end(),
-                  [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+    }
+}
+
+// Completes a collected batch (lock held).
+void finish(mgv_server* S, Inflight& sl) {
+    for (size_t i = 0; i < sl.reqs.size(); ++i) {
+        auto& q = sl.reqs[i];
         complete(S, q, sl.h_counts[i] > q->r.max_groups ? MGV_ENOMEM : MGV_OK);
         S->used -= q->bytes;
     }
@@ -255,7 +262,7 @@ mgv_status run_plain(mgv_server* S, Request& q) {
         if (st != MGV_OK) return st;
         S->plain_gb[r.max_groups] = gb;
     }
-    mgv_hash_probe_desc pd{0, 0, S->tables[r.table]};
+    mgv_hash_probe_desc pd{0, 0, q.table};
     if (st == MGV_OK) st = mgv_op_create_hash_probe(ctx, &pd, gb, &probe);
     mgv_select_desc sd{1, r.filter_bound};
     if (st == MGV_OK) st = mgv_op_create_select(ctx, &sd, probe, &sel);
@@ -290,11 +297,14 @@ void scheduler(mgv_server* S) {
             S->done_cv.notify_all();
             continue;
         }
-        // 1. harvest finished batches
+        // 1. harvest finished batches; the host copies run outside the lock
         bool any_busy = false;
         for (auto& sl : S->slots) {
             if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) {
-                harvest(S, sl);
+                lk.unlock();
+                collect(sl);
+                lk.lock();
+                finish(S, sl);
                 S->done_cv.notify_all();
             }
             any_busy |= sl.busy;
@@ -322,8 +332,13 @@ void scheduler(mgv_server* S) {
                 S->pending.pop_front();
             }
             if (!free_slot->reqs.empty()) {
+                lk.unlock();  // submitters and waiters go on while the batch is planned and launched
                 const mgv_status st = launch(S, *free_slot);
-                if (st != MGV_OK) {
+                lk.lock();
+                if (st == MGV_OK) {
+                    S->batches++;
+                    S->batched_queries += free_slot->reqs.size();
+                } else {
                     for (auto& q : free_slot->reqs) { S->used -= q->bytes; complete(S, q, st); }
                     free_slot->reqs.clear();
                     free_slot->busy = false;
@@ -401,6 +416,7 @@ mgv_status mgv_server_submit(mgv_server* S, const mgv_server_request* r, uint64_
         std::lock_guard<std::mutex> lk(S->mu);
         if (r->table >= S->tables.size()) return fail(MGV_EINVAL, "no such table");
         if (S->stop) return fail(MGV_ESTATE, "server is stopping");
+        q->table = S->tables[r->table];
         q->ticket = S->next_ticket++;
         S->by_ticket[q->ticket] = q;
         S->pending.push_back(q);
@@ -420,10 +436,13 @@ mgv_status mgv_server_wait(mgv_server* S, uint64_t ticket, uint32_t timeout_ms, 
     auto q = it->second;
     if (!S->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; }))
         return fail(MGV_ETIMEDOUT, "request not finished");
+    S->by_ticket.erase(it);
+    lk.unlock();  // the request is this caller's now: order and copy its rows outside the lock
+    std::sort(q->rows.begin(), q->rows.end(),
+              [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
     if (rows) *rows = q->rows.size();
     if (latency_ms) *latency_ms = q->latency_ms;
     if (out) std::copy(q->rows.begin(), q->rows.begin() + std::min<uint64_t>(cap, q->rows.size()), out);
-    S->by_ticket.erase(it);
     if (q->status != MGV_OK) return fail(q->status, "request failed");
     return MGV_OK;
 }

@@ -110,7 +110,8 @@ class QueryDesc(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("load_factor", c_float), ("build_item_rows", c_uint32), ("probe_item_rows", c_uint32),
-                ("probe_ctas_per_sm", c_uint32), ("use_graph", c_uint32), ("reserved", c_uint32 * 3)]
+                ("probe_ctas_per_sm", c_uint32), ("use_graph", c_uint32), ("item_order", c_uint32),
+                ("reserved", c_uint32 * 2)]
 
 
 class BatchStats(ctypes.Structure):

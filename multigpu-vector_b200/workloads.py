@@ -169,7 +169,11 @@ def run_batched(args, mgv, torch, ctx, bench, clk):
     nq = args.queries
     spec, descs, keep = _mix(ctx, torch, mgv, nq, 0x5EED0004, stream)
     t0 = time.perf_counter()
-    cfg = mgv.batch_autotune(ctx, descs)
+    if args.batch_config:
+        lf, items, order = args.batch_config.split(",")
+        cfg = mgv.BatchConfig(float(lf), 0, int(items), 0, 1, int(order))
+    else:
+        cfg = mgv.batch_autotune(ctx, descs)
     tune_s = time.perf_counter() - t0
     b = mgv.Batch(ctx, descs, cfg, keep)
     bt, pt = [], []
@@ -204,8 +208,8 @@ def run_batched(args, mgv, torch, ctx, bench, clk):
                      "how": "the same queries one at a time: hash_build open/consume/close, then "
                             "select->hash_probe->groupby open/consume/close, operators created once"},
            "speedup_vs_plain": tp / tb,
-           "autotuned": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
-                         "probe_ctas_per_sm": cfg.probe_ctas_per_sm, "tune_s": tune_s},
+           "batch_config": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
+                            "item_order": cfg.item_order, "autotuned": not args.batch_config, "tune_s": tune_s},
            "arena_bytes": st.arena_bytes, "probe_rows": rows,
            "probe_rows_per_s": rows / tb, "checked": "all queries equal between batched and plain"}, clk)
     b.destroy()
@@ -282,6 +286,9 @@ def run_served(args, mgv, torch, ctx, bench, clk):
         th.start()
         t0 = time.perf_counter()
         for a, (t, rows, bound) in zip(at, reqs):
+            wait = a - (time.perf_counter() - t0)
+            if wait > 1e-4:
+                time.sleep(wait - 5e-5)  # releases the GIL for the draining thread
             while time.perf_counter() - t0 < a:
                 pass
             nb, g, bk, cols = tables[t]
@@ -298,6 +305,7 @@ def run_served(args, mgv, torch, ctx, bench, clk):
                 "mean_ms": stats.mean_ms, "max_ms": stats.max_ms, "batches": stats.batches,
                 "mean_batch": stats.mean_batch, "peak_device_bytes": stats.peak_bytes}, digests
 
+    sys.setswitchinterval(2e-4)  # the submitting and draining threads share the GIL
     out = []
     h0 = time.time()
     for k, rate in enumerate(rates):

@@ -12,10 +12,10 @@ def descs(mgv, mix):
     return [mgv.query_desc(q["cols"][0], q["nb"], *q["cols"][1:], q["npr"], q["bound"], q["G"]) for q in mix]
 
 
-@pytest.mark.parametrize("use_graph", [0, 1])
-def test_batch_matches_plain_and_oracle(ctx, torch_cuda, use_graph):
+@pytest.mark.parametrize("use_graph,item_order", [(0, 0), (1, 0), (1, 1)])
+def test_batch_matches_plain_and_oracle(ctx, torch_cuda, use_graph, item_order):
     mix = make_mix(ctx, torch_cuda, 48, 11)
-    cfg = mgv.BatchConfig(0.5, 4096, 8192, 0, use_graph)
+    cfg = mgv.BatchConfig(0.5, 4096, 8192, 0, use_graph, item_order)
     b = mgv.Batch(ctx, descs(mgv, mix), cfg)
     b.run()
     b.run()  # second run: graph replay when use_graph
@@ -51,4 +51,24 @@ def test_autotune_picks_a_config(ctx, torch_cuda):
     b.run()
     for i, q in enumerate(mix):
         assert b.result(i) == oracle_answer(q), i
+    b.destroy()
+
+
+@pytest.mark.parametrize("item_order", [0, 1])
+def test_batch_ctas_switch_queries(ctx, torch_cuda, item_order):
+    """Hundreds of small queries: every CTA runs several queries in turn,
+    flushing one query's shared group table and loading the next query's
+    descriptor between them."""
+    mix = make_mix(ctx, torch_cuda, 600, 13, build=(6, 12), probe=(8, 13), groups=(2, 10))
+    cfg = mgv.BatchConfig(0.5, 4096, 8192, 1, 1, item_order)
+    b = mgv.Batch(ctx, descs(mgv, mix), cfg)
+    assert b.stats().probe_items > 2 * 148
+    for _ in range(3):
+        b.run()
+    b.run_plain()
+    for i, q in enumerate(mix):
+        got = b.result(i)
+        assert got == b.result(i, plain=True), i
+        if i % 5 == 0:
+            assert got == oracle_answer(q), i
     b.destroy()
