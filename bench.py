@@ -202,6 +202,7 @@ def main():
                     help="batched: 'load_factor,probe_item_rows,item_order' instead of autotuning")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="served: arrival window per rate")
     ap.add_argument("--rates", default="200,1000,5000", help="served: arrival rates (queries/s)")
+    ap.add_argument("--saturate", type=int, default=5000, help="served: requests in the closing burst")
     ap.add_argument("--gather-ceiling", action="store_true",
                     help="measure the random 32-byte bucket-read ceiling instead of the join")
     ap.add_argument("--settle-s", type=float, default=1.0, help="untimed steps before timing, in seconds")
