@@ -4,10 +4,12 @@
 //   * one device arena holds every query's join table, metadata, side list,
 //     group table, packed output region, and the descriptors and work-item
 //     lists the kernels read;
-//   * a run clears the tables (two fills and two memsets over contiguous
-//     regions), launches one persistent build kernel and one persistent probe
-//     kernel over (query, rows) items in query order, packs the groups, and
-//     copies the packed regions and their counts to pinned host memory;
+//   * a run clears the group tables (one fill and memsets over contiguous
+//     regions), builds every join table through shared memory (one set of
+//     region-build launches for all queries, which also writes the empty
+//     parts of the tables), launches one persistent probe kernel over
+//     (query, rows) items in query order, packs the groups, and copies the
+//     packed regions and their counts to pinned host memory;
 //   * with use_graph the run is captured once and replayed as a CUDA graph,
 //     so a run costs one graph launch and one synchronisation.
 // The plain baseline runs the same queries one at a time through the
@@ -45,7 +47,9 @@ struct mgv_batch {
     mgv_group_row* out_rows = nullptr;
     uint64_t out_rows_total = 0;
     ChainDev* d_qs = nullptr;
-    BatchBuild* d_builds = nullptr;
+    RegionJob* d_jobs = nullptr;  // one shared-memory build job per query
+    RegionScratch rsc{};
+    uint32_t total_regions = 0, max_job_regions = 0;
     BatchOut* d_outs = nullptr;
     BatchItem* d_build_items = nullptr;
     BatchItem* d_probe_items = nullptr;
@@ -97,14 +101,15 @@ void free_batch_device(mgv_batch* b) {
 mgv_status enqueue_run(mgv_batch* b, cudaStream_t s) {
     Context* ctx = b->ctx;
     MGV_CUDA_TRY(cudaMemsetAsync(ctx->d_err, 0, 2 * sizeof(uint32_t), s));
-    MGV_CUDA_TRY(launch_fill_u64(b->tables, b->table_words, kEmptySlot, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(b->metas, 0, 4 * sizeof(unsigned long long) * b->q.size(), s));
     MGV_CUDA_TRY(launch_fill_i32(b->group_keys, b->group_slots, kEmptyKey, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(b->group_zero, 0, b->group_zero_bytes, s));
     MGV_CUDA_TRY(cudaMemsetAsync(b->out_counts, 0, sizeof(uint32_t) * b->q.size(), s));
-    MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_builds, b->d_outs, b->d_build_items, b->n_build, b->d_probe_items,
-                              b->n_probe, b->d_compact_items, b->n_compact, (int)b->cfg.probe_ctas_per_sm,
-                              b->cfg.item_order, s, ctx));
+    // every region of every table is written by the build (no clearing pass)
+    MGV_CUDA_TRY(launch_build_regions(b->d_jobs, RegionJob{}, (uint32_t)b->q.size(), b->d_build_items, b->n_build, 0, 0,
+                                      b->total_regions, b->max_job_regions, b->rsc, true, s, ctx));
+    MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_outs, b->d_probe_items, b->n_probe, b->d_compact_items, b->n_compact,
+                              (int)b->cfg.probe_ctas_per_sm, b->cfg.item_order, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->out_counts, sizeof(uint32_t) * b->q.size(), cudaMemcpyDeviceToHost, s));
     if (b->out_rows_total)
         MGV_CUDA_TRY(cudaMemcpyAsync(b->h_rows, b->out_rows, sizeof(mgv_group_row) * b->out_rows_total,
@@ -197,7 +202,26 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     for (uint32_t i = 0; i < nq; ++i) { b->out_offset[i] = out_total; out_total += qs[i].max_groups; }
     const size_t rows_off = take(sizeof(mgv_group_row) * std::max<uint64_t>(out_total, 1));
     const size_t qs_off = take(sizeof(ChainDev) * std::max(nq, 1u));
-    const size_t builds_off = take(sizeof(BatchBuild) * std::max(nq, 1u));
+    const size_t jobs_off = take(sizeof(RegionJob) * std::max(nq, 1u));
+    std::vector<uint32_t> region0(nq);
+    uint32_t total_regions = 0, max_job_regions = 1;
+    uint64_t build_total = 0;
+    for (uint32_t i = 0; i < nq; ++i) {
+        const uint32_t r = (nbk[i] + kRegionBuckets - 1) / kRegionBuckets;
+        if (r > kMaxRegionsPerJob) {
+            delete b;
+            return fail(MGV_EUNSUPPORTED, "query " + std::to_string(i) + ": build side too large for a batch");
+        }
+        region0[i] = total_regions;
+        total_regions += r;
+        max_job_regions = std::max(max_job_regions, r);
+        build_total += qs[i].build_rows;
+    }
+    if (build_total >= (1ull << 31)) {
+        delete b;
+        return fail(MGV_EUNSUPPORTED, "a batch holds fewer than 2^31 build rows");
+    }
+    const size_t rsc_off = take(region_scratch_bytes(total_regions, build_total));
     const size_t outs_off = take(sizeof(BatchOut) * std::max(nq, 1u));
     // work items
     std::vector<BatchItem> bi, pi, ci;
@@ -236,7 +260,10 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     b->out_rows = reinterpret_cast<mgv_group_row*>(A + rows_off);
     b->out_rows_total = out_total;
     b->d_qs = reinterpret_cast<ChainDev*>(A + qs_off);
-    b->d_builds = reinterpret_cast<BatchBuild*>(A + builds_off);
+    b->d_jobs = reinterpret_cast<RegionJob*>(A + jobs_off);
+    b->rsc = carve_region_scratch(A + rsc_off, total_regions, build_total);
+    b->total_regions = total_regions;
+    b->max_job_regions = max_job_regions;
     b->d_outs = reinterpret_cast<BatchOut*>(A + outs_off);
     b->d_build_items = reinterpret_cast<BatchItem*>(A + bi_off);
     b->d_probe_items = reinterpret_cast<BatchItem*>(A + pi_off);
@@ -247,7 +274,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
 
     // ---- descriptors ----
     std::vector<ChainDev> hq(nq);
-    std::vector<BatchBuild> hb(nq);
+    std::vector<RegionJob> hj(nq);
     std::vector<BatchOut> ho(nq);
     for (uint32_t i = 0; i < nq; ++i) {
         TableView t{};
@@ -284,11 +311,12 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         c.nref = 2;
         c.gt = g;
         c.smem_groups = std::min(gcap[i], kMaxSmemGroups);
-        hb[i] = BatchBuild{qs[i].build_keys, qs[i].build_payloads, t};
+        hj[i] = RegionJob{t, qs[i].build_keys, qs[i].build_payloads, nullptr, 0, region0[i],
+                          (nbk[i] + kRegionBuckets - 1) / kRegionBuckets, 0};
         ho[i] = BatchOut{g, b->out_rows + b->out_offset[i], b->out_counts + i, qs[i].max_groups, 0};
     }
     e = cudaMemcpy(b->d_qs, hq.data(), sizeof(ChainDev) * nq, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(b->d_builds, hb.data(), sizeof(BatchBuild) * nq, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_jobs, hj.data(), sizeof(RegionJob) * nq, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_outs, ho.data(), sizeof(BatchOut) * nq, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !bi.empty())
         e = cudaMemcpy(b->d_build_items, bi.data(), sizeof(BatchItem) * bi.size(), cudaMemcpyHostToDevice);

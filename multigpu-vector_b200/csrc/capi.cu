@@ -539,6 +539,7 @@ mgv_status mgv_op_destroy(mgv_op* o) {
     cudaStreamSynchronize(o->ctx->stream);
     if (o->kind == OpKind::Sink) sink_return_buffers(o);
     if (o->h_res) cudaFreeHost(o->h_res);
+    if (o->rb_scratch) cudaFree(o->rb_scratch);
     for (void* p : o->allocs) cudaFree(p);
     delete o;
     return MGV_OK;
@@ -552,8 +553,10 @@ static mgv_status op_reset(Op* o, cudaStream_t s) {
             o->agg_result = mgv_agg_result{0, 0};
             break;
         case OpKind::HashBuild:
-            MGV_CUDA_TRY(launch_fill_u64(o->table.slots, 4ull * o->table.nbuckets, kEmptySlot, s, o->ctx));
+            // The table is cleared lazily: a first shared-memory build writes
+            // every bucket itself; otherwise the first consume (or close) fills it.
             MGV_CUDA_TRY(cudaMemsetAsync(o->table.meta, 0, 4 * sizeof(unsigned long long), s));
+            o->hb_fresh = true;
             o->unique = false;
             break;
         case OpKind::Sink: {
@@ -667,6 +670,10 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
     cudaStream_t s = pick_stream(o->ctx, stream);
     o->state = OpState::Closed;
     mgv_status st = MGV_OK;
+    if (o->kind == OpKind::HashBuild && o->hb_fresh) {  // nothing was built: clear the table now
+        MGV_CUDA_TRY(launch_fill_u64(o->table.slots, 4ull * o->table.nbuckets, kEmptySlot, s, o->ctx));
+        o->hb_fresh = false;
+    }
     if (!o->parent) {  // terminal: wait, check the device error word, read results
         if (o->kind == OpKind::Aggregate) {
             // one pinned landing zone, one synchronisation
@@ -879,8 +886,36 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
             const int32_t kc = (int32_t)term->hb.key_col, pc = term->hb.payload_col;
             if (!col_ok(kc) || (pc != -1 && !col_ok(pc))) return fail(MGV_EINVAL, "build column not in input");
             if (n == 0) return MGV_OK;
-            MGV_CUDA_TRY(launch_build(cols[kc], pc >= 0 ? cols[pc] : nullptr, sel ? cols[sel->sel.col] : nullptr,
-                                      sel ? sel->sel.bound : 0, sel != nullptr, n, term->table, s, ctx));
+            const int32_t* pays = pc >= 0 ? cols[pc] : nullptr;
+            const int32_t* filt = sel ? cols[sel->sel.col] : nullptr;
+            const int32_t bound = sel ? sel->sel.bound : 0;
+            const uint32_t regions = table_regions(term->table);
+            const bool fresh = term->hb_fresh;
+            term->hb_fresh = false;
+            if (n < kRegionBuildMinRows || n >= (1ull << 31) || regions > kMaxRegionsPerJob) {
+                if (fresh)
+                    MGV_CUDA_TRY(launch_fill_u64(term->table.slots, 4ull * term->table.nbuckets, kEmptySlot, s, ctx));
+                MGV_CUDA_TRY(launch_build(cols[kc], pays, filt, bound, sel != nullptr, n, term->table, s, ctx));
+                return MGV_OK;
+            }
+            // shared-memory build; its scratch is kept by the operator and grown on demand
+            const size_t need = region_scratch_bytes(regions, n);
+            if (term->rb_bytes < need) {
+                if (term->rb_scratch) {
+                    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+                    MGV_CUDA_TRY(cudaFree(term->rb_scratch));
+                    term->rb_scratch = nullptr;
+                    term->rb_bytes = 0;
+                }
+                MGV_CUDA_TRY(cudaMalloc(&term->rb_scratch, need));
+                term->rb_bytes = need;
+            }
+            const RegionJob job{term->table, cols[kc], pays, filt, bound, 0, regions, 0};
+            // items: two per SM, each worth zeroing and flushing its region histogram
+            const uint64_t rows_per_item =
+                std::max<uint64_t>({8ull * regions, 4096, n / (2ull * ctx->prop.multiProcessorCount) + 1});
+            MGV_CUDA_TRY(launch_build_regions(nullptr, job, 1, nullptr, 0, n, rows_per_item, regions, regions,
+                                              carve_region_scratch(term->rb_scratch, regions, n), fresh, s, ctx));
             return MGV_OK;
         }
         case OpKind::Partition: {

@@ -489,39 +489,6 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* 
     }
 }
 
-// Build phase of a batch: contiguous runs of (query, rows) items; every row
-// is inserted into its query's table.
-__global__ void __launch_bounds__(kChainBlock, 2) k_batch_build(const BatchBuild* __restrict__ bs,
-                                                                const BatchItem* __restrict__ items, uint32_t nitems,
-                                                                uint32_t item_order, uint32_t* err) {
-    const ItemRange r = item_range(nitems, item_order);
-    for (uint32_t it = r.first; it < r.end; it += r.step) {
-        const BatchItem item = items[it];
-        const BatchBuild& b = bs[item.q];
-        constexpr int R = kBuildRows;
-        bool dup = false;
-        uint32_t inserted = 0;
-        for (uint64_t i0 = item.lo + threadIdx.x; i0 < item.hi; i0 += (uint64_t)kChainBlock * R) {
-            int32_t k[R], p[R];
-            bool valid[R];
-#pragma unroll
-            for (int j = 0; j < R; ++j) {
-                const uint64_t i = i0 + (uint64_t)j * kChainBlock;
-                valid[j] = i < item.hi;
-                k[j] = valid[j] ? __ldg(b.keys + i) : 0;
-                p[j] = (valid[j] && b.pays) ? __ldg(b.pays + i) : 0;
-            }
-            table_insert_rows<R>(b.table, k, p, valid, err, dup, inserted);
-        }
-        const unsigned long long tot = warp_sum_u64(inserted);
-        const unsigned any_dup = __any_sync(0xffffffffu, dup);
-        if (lane_id() == 0) {
-            if (tot) atomicAdd(b.table.meta + 2, tot);
-            if (any_dup) atomicOr(b.table.meta + 3, 1ull);
-        }
-    }
-}
-
 // Packs each query's groups into its output region (unsorted) and counts them.
 __global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchItem* __restrict__ items,
                                 uint32_t nitems, uint32_t* err) {
@@ -548,20 +515,10 @@ __global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchIt
     }
 }
 
-cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
-                         const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
+cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const BatchItem* probe_items, uint32_t n_probe,
                          const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
                          cudaStream_t s, Context* ctx) {
     const int sms = ctx->prop.multiProcessorCount;
-    if (n_build) {
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_build, kChainBlock, 0);
-        const int grid = (int)std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * sms, n_build);
-        k_batch_build<<<grid, kChainBlock, 0, s>>>(d_builds, build_items, n_build, item_order, ctx->d_err);
-        ctx->launches++;
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
     if (n_probe) {
         const size_t smem = kRingBytes + smem_groups_bytes(kMaxSmemGroups);
         cudaError_t e = cudaFuncSetAttribute(k_batch_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -162,6 +162,10 @@ struct Op {
     unsigned long long* pt_dev = nullptr; // [P] histogram / cursors
     std::vector<uint64_t> pt_hist;        // rows per partition (all runs)
     std::vector<std::pair<uint64_t, uint64_t>> pt_runs;  // (first row, rows)
+    bool hb_fresh = false;  // opened, nothing consumed yet: the table is not cleared yet
+    // shared-memory build scratch (hash_build), grown on demand
+    void* rb_scratch = nullptr;
+    size_t rb_bytes = 0;
     // device allocations owned by this op
     std::vector<void*> allocs;
 };
@@ -246,11 +250,44 @@ struct BatchItem {  // rows [lo, hi) of query q
     uint32_t pad;
     uint64_t lo, hi;
 };
-struct BatchBuild {  // build side of a query
+// Shared-memory hash-table build (build_regions.cu).  A table is cut into
+// regions of kRegionBuckets buckets; build rows are bucketed by the region of
+// their home bucket, then one CTA per region inserts the region's rows into
+// a shared-memory copy of the region and writes it back with coalesced
+// stores.  A row whose run leaves its region is inserted afterwards into the
+// global table.  A "job" is one table's build; a launch can build many.
+constexpr uint32_t kRegionBuckets = 2048;      // 64 KiB of table per region
+constexpr uint32_t kMaxRegionsPerJob = 16384;  // per-CTA region histogram: 64 KiB
+constexpr uint64_t kRegionBuildMinRows = 1u << 16;  // smaller builds: one global CAS per row
+struct RegionJob {
+    TableView t;
     const int32_t* keys;
-    const int32_t* pays;
-    TableView table;
+    const int32_t* pays;      // nullable
+    const int32_t* filt;      // nullable: rows with filt <= bound only
+    int32_t bound;
+    uint32_t region0;         // first region of this job in the launch
+    uint32_t nregions;
+    uint32_t pad;
 };
+struct RegionScratch {
+    uint32_t* hist;           // [regions] rows per region
+    uint32_t* start;          // [regions + 1] first staging row of each region
+    uint32_t* cursor;         // [regions]
+    uint32_t* ovf_count;      // [1]
+    unsigned long long* staging;  // [rows] {key, payload}, region-major
+    unsigned long long* ovf;  // [rows] job << 32 | staging row, left for the global insert
+};
+inline uint32_t table_regions(const TableView& t) { return (t.nbuckets + kRegionBuckets - 1) / kRegionBuckets; }
+size_t region_scratch_bytes(uint32_t regions, uint64_t rows);
+RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows);
+// Items: explicit (job, rows) items, or (items == nullptr) rows [0, n) of
+// job0 cut into items of rows_per_item.  fresh: the tables hold nothing yet
+// and are not cleared beforehand; every region is written.
+cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0, uint32_t njobs,
+                                 const struct BatchItem* items, uint32_t nitems, uint64_t n, uint64_t rows_per_item,
+                                 uint32_t total_regions, uint32_t max_job_regions, const RegionScratch& sc,
+                                 bool fresh, cudaStream_t s, Context* ctx);
+
 struct BatchOut {  // packed result region of a query
     GroupTableView gt;
     mgv_group_row* rows;
@@ -258,8 +295,7 @@ struct BatchOut {  // packed result region of a query
     uint32_t capacity;
     uint32_t pad;
 };
-cudaError_t launch_batch(const ChainDev* d_qs, const BatchBuild* d_builds, const BatchOut* d_outs,
-                         const BatchItem* build_items, uint32_t n_build, const BatchItem* probe_items, uint32_t n_probe,
+cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const BatchItem* probe_items, uint32_t n_probe,
                          const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
                          cudaStream_t s, Context* ctx);
 

@@ -211,8 +211,7 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     MGV_CUDA_TRY(launch_fill_i32(reinterpret_cast<int32_t*>(A), slots, kEmptyKey, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(A + zero_begin, 0, zero_end - zero_begin, s));
     MGV_CUDA_TRY(cudaMemsetAsync(A + counts_off, 0, 4ull * nq, s));
-    MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), nullptr,
-                              reinterpret_cast<BatchOut*>(A + outs_off), nullptr, 0,
+    MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), reinterpret_cast<BatchOut*>(A + outs_off),
                               reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(),
                               reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, 0u, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));

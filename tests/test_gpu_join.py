@@ -277,3 +277,45 @@ def test_staged_probe_is_repeatable(ctx, torch_cuda, tuned):
         assert agg.result() == want
     for o in (probe, agg, hb):
         o.destroy()
+
+
+@pytest.mark.parametrize("lf,build_filter", [(0.5, None), (0.95, None), (0.75, 50000)])
+def test_shared_memory_build(ctx, torch_cuda, lf, build_filter):
+    """Builds of 2^16 rows or more go through the shared-memory region build.
+    Duplicate keys, 20000 copies of one key (a run that crosses region ends,
+    so rows are finished by the global overflow insert), INT32_MIN rows, a
+    build-side filter and two consume calls into the same table."""
+    mn = -(1 << 31)
+    nb, npb = 300000, 400000
+    bk = po.gen_uniform(nb, 0x5EED0603, 0, 0, 60000)
+    bk[:20000] = 7
+    bk[20000:20010] = mn
+    bp = po.gen_uniform(nb, 0x5EED0603, 1, -(1 << 31), 1 << 32)
+    pk = po.gen_uniform(npb, 0x5EED0603, 2, -100, 60100)
+    pk[:500] = 7
+    pk[500:505] = mn
+    pp = po.gen_uniform(npb, 0x5EED0603, 3, -(1 << 31), 1 << 32)
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb, lf, build_filter)
+    bhead.open()
+    half = nb // 2
+    bhead.consume_columns([dev(torch_cuda, bk[:half]), dev(torch_cuda, bp[:half])], half)
+    bhead.consume_columns([dev(torch_cuda, bk[half:]), dev(torch_cuda, bp[half:])], nb - half)
+    bhead.close()
+    info = hb.result()
+    probe.open()
+    probe.consume_columns([dev(torch_cuda, pk), dev(torch_cuda, pp)], npb)
+    probe.close()
+    keep = np.ones(nb, bool) if build_filter is None else bk <= build_filter
+    assert agg.result() == po.Chain(bk[keep], bp[keep]).probe_agg(pk, pp)
+    assert info.rows == int(keep.sum()) and info.reserved_key_rows == 10 and info.has_duplicates == 1
+    for o in (probe, agg, bhead, hb):
+        o.destroy()
+
+
+def test_shared_memory_build_unique_keys(ctx, torch_cuda):
+    """A region-built table of unique keys is reported duplicate-free (so the
+    probe stops at the first match) and joins exactly."""
+    bk, bp, pk, pp, hits = config2_inputs(1 << 20, 1 << 21)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
+    assert info.has_duplicates == 0 and info.rows == 1 << 20
+    assert cnt == hits and (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
