@@ -231,17 +231,10 @@ def main():
         ctx.close()
         return 0
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
+    import replicas
 
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist, world, rank, local = replicas.init("nccl")
     torch.cuda.set_device(local)
     ctx = mgv.Context(local)
     tune = {k: v for k, v in (("probe_kernel", args.probe_kernel), ("probe_rows_per_thread", args.rows_per_thread),
@@ -313,10 +306,8 @@ def main():
         dist.barrier()
     elapsed = start.elapsed_time(end) / 1000.0
     kernel_s = statistics.mean(a.elapsed_time(b) for a, b in kev) / 1000.0
-    if dist:
-        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = replicas.max_over_ranks(dist, elapsed, "cuda")
+    assert replicas.same_on_all_ranks(dist, (cnt, s)), "replicas disagree"
     # ---- end to end through the C ABI from pinned host memory -------------
     e2e = None
     if not args.no_e2e:
@@ -367,12 +358,10 @@ def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world,
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_s = e0.elapsed_time(e1) / 1000.0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * npb * e2e_steps / e2e_s
+    import replicas
+
+    e2e_s = replicas.max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0, "cuda")
+    e2e_value = replicas.job_rate(world, npb * e2e_steps, e2e_s)
     for b in bufs:
         pool.release(b)
     pool.destroy()
@@ -382,7 +371,9 @@ def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world,
 
 def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank, dist,
            ops, nb, npb, tuning):
-    value = world * npb * args.steps / elapsed
+    import replicas
+
+    value = replicas.job_rate(world, npb * args.steps, elapsed)
     peak, peak_kind = measured_peaks()
     achieved = BYTES_PER_TUPLE * npb / kernel_s / 1e9
     line = {
@@ -414,9 +405,7 @@ def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, 
     for o in ops:
         o.destroy()
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     return 0
 
 

@@ -40,7 +40,8 @@ def _line(args, metric, value, unit, ms, workload, extra, clk, higher=True):
          "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": {"workload": workload}}
     d.update(extra)
     d["clocks"] = clk.summary()
-    print(json.dumps(d), flush=True)
+    if int(os.environ.get("RANK", "0")) == 0:  # under torchrun every rank runs its own replica
+        print(json.dumps(d), flush=True)
 
 
 def run_select(args, mgv, torch, ctx, bench, clk):
