@@ -422,7 +422,9 @@ mgv_status mgv_server_create(mgv_ctx *ctx, const mgv_server_config *cfg, mgv_ser
 mgv_status mgv_server_add_table(mgv_server *s, const int32_t *keys, const int32_t *payloads, uint64_t rows,
                                 uint32_t *table_id);
 mgv_status mgv_server_submit(mgv_server *s, const mgv_server_request *r, uint64_t *ticket);
-/* Waits (bounded by timeout_ms) for a request; its groups sorted by group. */
+/* Waits (bounded by timeout_ms) for a request and copies up to cap of its
+ * groups to out, in no particular order (as GROUP BY defines); *rows = the
+ * number of groups. */
 mgv_status mgv_server_wait(mgv_server *s, uint64_t ticket, uint32_t timeout_ms, mgv_group_row *out,
                            uint64_t cap, uint64_t *rows, double *latency_ms);
 mgv_status mgv_server_stats_get(mgv_server *s, mgv_server_stats *out);

@@ -186,6 +186,16 @@ __device__ __forceinline__ uint32_t job_of_region(const RegionJob* jobs, uint32_
     return lo;
 }
 
+// 16-byte shared-memory read, issued where it stands (not cached across CAS).
+__device__ __forceinline__ uint4 lds_v4(const void* p) {
+    uint4 r;
+    asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "r"(smem_u32(p))
+                 : "memory");
+    return r;
+}
+
 // Inserts one staged row into the shared region (linear probing inside it).
 // A slot is claimed with a 32-bit CAS on its key word, then its payload word
 // is stored: nothing reads payloads before the region is written back.
@@ -194,14 +204,17 @@ __device__ __forceinline__ bool region_insert(unsigned long long* tab, uint32_t 
     const uint32_t key = (uint32_t)v;
     uint32_t* words = reinterpret_cast<uint32_t*>(tab);  // slot q of bucket b: words[8b + 2q] key, +1 payload
     for (; b < nb; ++b) {
+        // the whole bucket in two 16-byte reads; a stale empty key only costs a failed CAS
+        const uint4 s01 = lds_v4(words + 8 * b);
+        const uint4 s23 = lds_v4(words + 8 * b + 4);
+        const uint32_t ks[4] = {s01.x, s01.z, s23.x, s23.z};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            uint32_t* kw = words + 8 * b + 2 * q;
-            uint32_t c = *(volatile uint32_t*)kw;
+            uint32_t c = ks[q];
             if (c == (uint32_t)kEmptyKey) {
-                c = atomicCAS(kw, (uint32_t)kEmptyKey, key);
+                c = atomicCAS(words + 8 * b + 2 * q, (uint32_t)kEmptyKey, key);
                 if (c == (uint32_t)kEmptyKey) {
-                    kw[1] = (uint32_t)(v >> 32);
+                    words[8 * b + 2 * q + 1] = (uint32_t)(v >> 32);
                     return true;
                 }
             }
@@ -249,7 +262,10 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
                 bulk_g2s(tab, gslots, nb * 32, &bar);
             }
             if (!mbar_wait_bounded(&bar, phase, 1u << 24)) {
-                if (threadIdx.x == 0) set_error(err, kDevTimeout, 40);
+                if (threadIdx.x == 0) {
+                    set_error(err, kDevTimeout, 40);
+                    bulk_wait_all();
+                }
                 return;
             }
             phase ^= 1u;
@@ -277,7 +293,8 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
         __syncthreads();
         if (threadIdx.x == 0) {
             bulk_s2g(gslots, tab, nb * 32);
-            bulk_commit_and_wait_all();
+            bulk_commit();
+            bulk_wait_reads();  // the buffer may be refilled; the write itself completes in the background
         }
         const unsigned long long tot = warp_sum_u64(ins);
         const bool any_dup = __any_sync(0xffffffffu, dup);
@@ -286,6 +303,7 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
             if (any_dup) atomicOr(sj.t.meta + 3, 1ull);
         }
     }
+    if (threadIdx.x == 0) bulk_wait_all();  // every region store is complete before the CTA ends
 }
 
 // Rows whose run left their region, into the global table (each entry:

@@ -73,6 +73,36 @@ static mgv_status check_device(Context* ctx, cudaStream_t s) {
 
 static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n, cudaStream_t s);
 
+// A terminal group-by's close: its groups are packed on the device and come
+// back with the error word in one copy to pinned memory and one
+// synchronisation, then are ordered by group.
+static mgv_status close_groupby(Op* o, cudaStream_t s) {
+    Context* ctx = o->ctx;
+    unsigned char* h = o->gb_land;
+    MGV_CUDA_TRY(cudaMemsetAsync(o->gb_dev_count, 0, sizeof(uint32_t), s));
+    MGV_CUDA_TRY(launch_group_pack(o->gtab, o->gb_dev_rows, o->gb_dev_count, s, ctx));
+    MGV_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(h + 8, o->gb_dev_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(h + 16, o->gb_dev_rows, sizeof(mgv_group_row) * (size_t)o->gb_land_rows,
+                                 cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
+    mgv_status st = report_device_error(ctx, w, s);
+    if (st != MGV_OK) return st;
+    uint32_t n = 0;
+    std::memcpy(&n, h + 8, sizeof(n));
+    const mgv_group_row* rows = reinterpret_cast<const mgv_group_row*>(h + 16);
+    o->gb_rows.assign(rows, rows + std::min(n, o->gb_land_rows));
+    if (n > o->gb_land_rows) {  // more groups than the landing zone holds
+        o->gb_rows.resize(n);
+        MGV_CUDA_TRY(cudaMemcpy(o->gb_rows.data() + o->gb_land_rows, o->gb_dev_rows + o->gb_land_rows,
+                                sizeof(mgv_group_row) * (size_t)(n - o->gb_land_rows), cudaMemcpyDeviceToHost));
+    }
+    std::sort(o->gb_rows.begin(), o->gb_rows.end(),
+              [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+    return MGV_OK;
+}
+
 extern "C" {
 
 const char* mgv_status_string(mgv_status s) {
@@ -467,6 +497,13 @@ mgv_status mgv_op_create_groupby(mgv_ctx* ctx, const mgv_groupby_desc* d, mgv_op
     if (st == MGV_OK) st = dev_alloc(o, (void**)&g.sums, sizeof(unsigned long long) * cap);
     if (st == MGV_OK) st = dev_alloc(o, (void**)&g.counts, sizeof(unsigned long long) * cap);
     if (st == MGV_OK) st = dev_alloc(o, (void**)&g.special, 2 * sizeof(unsigned long long));
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&o->gb_dev_rows, sizeof(mgv_group_row) * ((size_t)cap + 1));
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&o->gb_dev_count, sizeof(uint32_t));
+    // pinned landing zone: results of up to 64 Ki groups come back with one synchronisation
+    o->gb_land_rows = std::min<uint32_t>(cap + 1, 1u << 16);
+    if (st == MGV_OK &&
+        cudaMallocHost(&o->gb_land, 16 + sizeof(mgv_group_row) * (size_t)o->gb_land_rows) != cudaSuccess)
+        st = fail(MGV_ENOMEM, "pinned host allocation");
     if (st != MGV_OK) {
         for (void* p : o->allocs) cudaFree(p);
         delete o;
@@ -540,6 +577,7 @@ mgv_status mgv_op_destroy(mgv_op* o) {
     if (o->kind == OpKind::Sink) sink_return_buffers(o);
     if (o->h_res) cudaFreeHost(o->h_res);
     if (o->rb_scratch) cudaFree(o->rb_scratch);
+    if (o->gb_land) cudaFreeHost(o->gb_land);
     for (void* p : o->allocs) cudaFree(p);
     delete o;
     return MGV_OK;
@@ -627,24 +665,7 @@ static mgv_status op_finish(Op* o, cudaStream_t s) {
             o->unique = m[3] == 0;
             break;
         }
-        case OpKind::Groupby: {
-            const uint32_t cap = o->gtab.cap;
-            std::vector<int32_t> keys(cap);
-            std::vector<unsigned long long> sums(cap), counts(cap), special(2);
-            MGV_CUDA_TRY(cudaMemcpyAsync(keys.data(), o->gtab.keys, sizeof(int32_t) * cap, cudaMemcpyDeviceToHost, s));
-            MGV_CUDA_TRY(cudaMemcpyAsync(sums.data(), o->gtab.sums, 8ull * cap, cudaMemcpyDeviceToHost, s));
-            MGV_CUDA_TRY(cudaMemcpyAsync(counts.data(), o->gtab.counts, 8ull * cap, cudaMemcpyDeviceToHost, s));
-            MGV_CUDA_TRY(cudaMemcpyAsync(special.data(), o->gtab.special, 16, cudaMemcpyDeviceToHost, s));
-            MGV_CUDA_TRY(cudaStreamSynchronize(s));
-            o->gb_rows.clear();
-            if (special[1]) o->gb_rows.push_back(mgv_group_row{kEmptyKey, 0, (int64_t)special[0], (int64_t)special[1]});
-            for (uint32_t i = 0; i < cap; ++i)
-                if (keys[i] != kEmptyKey && counts[i])
-                    o->gb_rows.push_back(mgv_group_row{keys[i], 0, (int64_t)sums[i], (int64_t)counts[i]});
-            std::sort(o->gb_rows.begin(), o->gb_rows.end(),
-                      [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
-            break;
-        }
+        case OpKind::Groupby: break;  // read back by close_groupby()
         case OpKind::Sink: {
             unsigned long long rows = 0;
             MGV_CUDA_TRY(cudaMemcpyAsync(&rows, o->sink.cursor, sizeof(rows), cudaMemcpyDeviceToHost, s));
@@ -686,6 +707,7 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
             o->agg_result.sum = (int64_t)h[3];
             return report_device_error(o->ctx, w, s);
         }
+        if (o->kind == OpKind::Groupby) return close_groupby(o, s);
         st = check_device(o->ctx, s);
         mgv_status st2 = op_finish(o, s);
         if (st == MGV_OK) st = st2;

@@ -169,12 +169,20 @@ struct SmemGroups {
     uint32_t* cnt;
     uint32_t* lo;
     uint32_t* hi;
-    uint32_t cap;  // power of two, 0 = no shared table
+    uint32_t* used;  // slots claimed so far
+    uint32_t cap;    // power of two, 0 = no shared table
 };
 
 constexpr uint32_t kGroupProbes = 16;  // shared-table probes before a row goes to the global table
 
-__host__ __device__ __forceinline__ size_t smem_groups_bytes(uint32_t cap) { return cap ? (size_t)(cap + 1) * 16 : 0; }
+// New groups are admitted to the shared table until it is this full; later
+// ones go to the global table, so a lookup that misses ends at an empty slot
+// after a few probes instead of scanning a crowded table.
+__host__ __device__ __forceinline__ uint32_t smem_groups_limit(uint32_t cap) { return cap - cap / 4 - cap / 8; }
+
+__host__ __device__ __forceinline__ size_t smem_groups_bytes(uint32_t cap) {
+    return cap ? (size_t)(cap + 1) * 16 + 16 : 0;
+}
 
 __device__ __forceinline__ SmemGroups smem_groups_at(unsigned char* base, uint32_t cap) {
     SmemGroups sg;
@@ -182,6 +190,7 @@ __device__ __forceinline__ SmemGroups smem_groups_at(unsigned char* base, uint32
     sg.cnt = reinterpret_cast<uint32_t*>(base) + (cap + 1);
     sg.lo = reinterpret_cast<uint32_t*>(base) + 2 * (cap + 1);
     sg.hi = reinterpret_cast<uint32_t*>(base) + 3 * (cap + 1);
+    sg.used = reinterpret_cast<uint32_t*>(base) + 4 * (cap + 1);
     sg.cap = cap;
     return sg;
 }
@@ -197,7 +206,11 @@ __device__ __forceinline__ void group_add_row(const SmemGroups& sg, const GroupT
 #pragma unroll 1
             for (uint32_t i = 0; i < kGroupProbes; ++i) {
                 int32_t k = *((volatile int32_t*)(sg.keys + slot));
-                if (k == kEmptyKey) k = atomicCAS(sg.keys + slot, kEmptyKey, g);
+                if (k == kEmptyKey) {
+                    if (*(volatile uint32_t*)sg.used >= smem_groups_limit(sg.cap)) break;  // stays global
+                    k = atomicCAS(sg.keys + slot, kEmptyKey, g);
+                    if (k == kEmptyKey) atomicAdd(sg.used, 1u);
+                }
                 if (k == kEmptyKey || k == g) {
                     hit = true;
                     break;
@@ -223,6 +236,7 @@ __device__ __forceinline__ void smem_groups_init(const SmemGroups& sg) {
         sg.lo[i] = 0;
         sg.hi[i] = 0;
     }
+    if (threadIdx.x == 0) *sg.used = 0;
 }
 
 __device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const GroupTableView& gt, uint32_t* err) {
@@ -315,59 +329,66 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
 #pragma unroll
             for (int j = 0; j < 4; ++j) emit(in[j], j, 0);
         } else {
-            // home-bucket loads of all four rows first, then walk each run
+            // Rounds over the four rows' runs: every round examines one bucket
+            // per row still walking and emits its matches; the rows whose run
+            // continues past a full bucket then load their next buckets
+            // together, so a round costs one memory latency for all of them.
+            const unsigned long long* __restrict__ slots = a.table.slots;
+            const uint32_t nbuckets = a.table.nbuckets;
             uint32_t w[4][8];
-            uint32_t hb[4];
+            uint32_t b[4];
             int32_t key[4];
+            bool live[4];
+            bool reserved_any = false;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 key[j] = pick_slot<NS>(v, a.probe_slot, j);
-                hb[j] = home_bucket(key[j], a.table);
-                if (in[j] && key[j] != kEmptyKey) ld_bucket(a.table.slots + 4ull * hb[j], w[j]);
+                live[j] = in[j] && key[j] != kEmptyKey;
+                reserved_any |= in[j] && key[j] == kEmptyKey;
+                b[j] = home_bucket(key[j], a.table);
+                if (live[j]) ld_bucket(slots + 4ull * b[j], w[j]);
             }
-            const uint32_t side_n =
-                (uint32_t)min((unsigned long long)a.table.meta[0], (unsigned long long)a.table.side_cap);
+            if (__any_sync(0xffffffffu, reserved_any)) {  // INT32_MIN keys join every side-list row
+                const uint32_t side_n =
+                    (uint32_t)min((unsigned long long)a.table.meta[0], (unsigned long long)a.table.side_cap);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                uint32_t wb[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) wb[q] = w[j][q];
-                uint32_t b = hb[j], slot = 0, side_i = 0;
-                const bool reserved = in[j] && key[j] == kEmptyKey;
-                bool done = !in[j] || reserved;
-                bool side_done = !reserved;
-                for (uint32_t guard = 0;; ++guard) {
-                    const bool more_any = __any_sync(0xffffffffu, !done || !side_done);
-                    if (!more_any || guard > a.table.nbuckets * 5u + side_n + 8u) break;
-                    bool found = false;
-                    int32_t bp = 0;
-                    if (!side_done) {
-                        if (side_i < side_n) {
-                            found = true;
-                            bp = a.table.side_pay[side_i++];
-                        }
-                        if (side_i >= side_n) side_done = true;
-                    } else if (!done) {
-#pragma unroll
-                        for (uint32_t q = 0; q < 4; ++q) {
-                            if (!found && q >= slot && wb[2 * q] == (uint32_t)key[j]) {
-                                found = true;
-                                bp = (int32_t)wb[2 * q + 1];
-                                slot = q + 1;
-                            }
-                        }
-                        if (found) {
-                            if (unique) done = true;
-                        } else if (wb[6] != (uint32_t)kEmptyKey) {  // run continues
-                            b = (b + 1 == a.table.nbuckets) ? 0u : b + 1;
-                            slot = 0;
-                            ld_bucket(a.table.slots + 4ull * b, wb);
-                        } else {
-                            done = true;
-                        }
-                    }
-                    emit(found, j, bp);
+                for (int j = 0; j < 4; ++j) {
+                    const bool r = in[j] && key[j] == kEmptyKey;
+                    if (__any_sync(0xffffffffu, r))
+                        for (uint32_t i = 0; i < side_n; ++i) emit(r, j, a.table.side_pay[i]);
                 }
+            }
+            for (uint32_t round = 0; round <= nbuckets; ++round) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint32_t k = (uint32_t)key[j];
+                    if (unique) {  // at most one match per run
+                        bool f = false;
+                        int32_t bp = 0;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            if (live[j] && !f && w[j][2 * q] == k) {
+                                f = true;
+                                bp = (int32_t)w[j][2 * q + 1];
+                            }
+                        if (__any_sync(0xffffffffu, f)) emit(f, j, bp);
+                        live[j] = live[j] && !f && w[j][6] != (uint32_t)kEmptyKey;
+                    } else {  // every match of the run
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const bool m = live[j] && w[j][2 * q] == k;
+                            if (__any_sync(0xffffffffu, m)) emit(m, j, (int32_t)w[j][2 * q + 1]);
+                        }
+                        live[j] = live[j] && w[j][6] != (uint32_t)kEmptyKey;
+                    }
+                }
+                if (!__any_sync(0xffffffffu, live[0] || live[1] || live[2] || live[3])) break;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (live[j]) {
+                        b[j] = (b[j] + 1 == nbuckets) ? 0u : b[j] + 1;
+                        ld_bucket(slots + 4ull * b[j], w[j]);
+                    }
             }
         }
         __syncwarp();
@@ -410,7 +431,7 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_chain(ChainDev a, uint32_t* 
     const uint32_t warp = threadIdx.x / 32;
     // shared layout: [id rings | group table]
     uint32_t* rings = reinterpret_cast<uint32_t*>(smem_raw);
-    SmemGroups sg{nullptr, nullptr, nullptr, nullptr, 0};
+    SmemGroups sg{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
     if (TERM == kTermGroupby && a.smem_groups) {
         sg = smem_groups_at(smem_raw + kRingBytes, a.smem_groups);
         smem_groups_init(sg);
@@ -456,7 +477,7 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* 
     static_assert(sizeof(ChainDev) % 4 == 0, "ChainDev is copied as 32-bit words");
     const uint32_t warp = threadIdx.x / 32;
     uint32_t* rings = reinterpret_cast<uint32_t*>(smem_raw);
-    const SmemGroups no_sg{nullptr, nullptr, nullptr, nullptr, 0};
+    const SmemGroups no_sg{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
     SmemGroups sg = no_sg;
 
     const ItemRange r = item_range(nitems, item_order);
@@ -513,6 +534,41 @@ __global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchIt
             o.rows[pos] = r;
         }
     }
+}
+
+// Packs the non-empty groups of a global group table (the group INT32_MIN
+// included) into out[0 .. *count); one warp-aggregated reservation per warp.
+__global__ void k_group_pack(GroupTableView gt, mgv_group_row* __restrict__ out, uint32_t* count) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t end = ((uint64_t)gt.cap + 1 + 31) & ~31ull;  // whole warps take part in the ballots
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+        const bool special = i == gt.cap;
+        bool keep = false;
+        mgv_group_row r{};
+        if (i <= gt.cap) {
+            r.group = special ? kEmptyKey : gt.keys[i];
+            const unsigned long long c = special ? gt.special[1] : gt.counts[i];
+            keep = c != 0 && (special || r.group != kEmptyKey);
+            if (keep) {
+                r.sum = (int64_t)(special ? gt.special[0] : gt.sums[i]);
+                r.count = (int64_t)c;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        uint32_t base = 0;
+        if (lane_id() == 0 && m) base = atomicAdd(count, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (keep) out[base + __popc(m & ((1u << lane_id()) - 1u))] = r;
+    }
+}
+
+cudaError_t launch_group_pack(const GroupTableView& gt, mgv_group_row* out, uint32_t* count, cudaStream_t s,
+                              Context* ctx) {
+    const uint64_t want = ((uint64_t)gt.cap + 1 + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->prop.multiProcessorCount * 8;
+    k_group_pack<<<(int)(want < cap ? want : cap), 256, 0, s>>>(gt, out, count);
+    ctx->launches++;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const BatchItem* probe_items, uint32_t n_probe,

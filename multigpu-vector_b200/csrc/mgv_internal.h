@@ -154,6 +154,10 @@ struct Op {
     mgv_groupby_desc gb{};
     GroupTableView gtab{};
     std::vector<mgv_group_row> gb_rows;
+    mgv_group_row* gb_dev_rows = nullptr;  // [cap + 1] packed by close()
+    uint32_t* gb_dev_count = nullptr;
+    unsigned char* gb_land = nullptr;      // pinned: {err[2], count, pad} then kGroupLandRows rows
+    uint32_t gb_land_rows = 0;
     // partition
     mgv_partition_desc pt{};
     int32_t* pt_store = nullptr;          // ncols x capacity, partition-major runs
@@ -295,6 +299,8 @@ struct BatchOut {  // packed result region of a query
     uint32_t capacity;
     uint32_t pad;
 };
+cudaError_t launch_group_pack(const GroupTableView& gt, mgv_group_row* out, uint32_t* count, cudaStream_t s,
+                              Context* ctx);
 cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const BatchItem* probe_items, uint32_t n_probe,
                          const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
                          cudaStream_t s, Context* ctx);

@@ -21,7 +21,8 @@ namespace mgv {
 namespace {
 
 constexpr int kPartBlock = 256;
-constexpr int kPartRows = 4;  // rows per thread per tile
+constexpr int kPartRows = 16;  // rows per thread per tile: one reservation per partition per 4096 rows
+constexpr int kHistRows = 8;   // histogram: key loads per thread in flight
 
 template <bool SEL>
 __global__ void __launch_bounds__(kPartBlock)
@@ -30,9 +31,20 @@ __global__ void __launch_bounds__(kPartBlock)
     extern __shared__ uint32_t sh[];
     for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock) sh[p] = 0;
     __syncthreads();
-    for (uint64_t i = (uint64_t)blockIdx.x * kPartBlock + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kPartBlock) {
-        if (SEL && !(__ldg(filt + i) <= bound)) continue;
-        atomicAdd(&sh[((uint32_t)__ldg(keys + i) >> shift) & mask], 1u);
+    const uint64_t stride = (uint64_t)gridDim.x * kPartBlock;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * kPartBlock + threadIdx.x; i0 < n; i0 += stride * kHistRows) {
+        int32_t k[kHistRows];
+        bool in[kHistRows];
+#pragma unroll
+        for (int u = 0; u < kHistRows; ++u) {
+            const uint64_t i = i0 + u * stride;
+            in[u] = i < n;
+            k[u] = in[u] ? __ldg(keys + i) : 0;
+            if (SEL && in[u]) in[u] = __ldg(filt + i) <= bound;
+        }
+#pragma unroll
+        for (int u = 0; u < kHistRows; ++u)
+            if (in[u]) atomicAdd(&sh[((uint32_t)k[u] >> shift) & mask], 1u);
     }
     __syncthreads();
     for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock)
@@ -44,7 +56,7 @@ struct ScatterCols {
 };
 
 template <bool SEL>
-__global__ void __launch_bounds__(kPartBlock)
+__global__ void __launch_bounds__(kPartBlock, 2)
     k_part_scatter(ScatterCols in, uint32_t ncols, uint32_t key_col, const int32_t* __restrict__ filt, int32_t bound,
                    uint64_t n, uint32_t shift, uint32_t mask, unsigned long long* cursors, int32_t* out,
                    uint64_t out_stride) {

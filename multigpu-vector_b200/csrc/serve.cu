@@ -436,9 +436,7 @@ mgv_status mgv_server_wait(mgv_server* S, uint64_t ticket, uint32_t timeout_ms, 
     if (!S->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; }))
         return fail(MGV_ETIMEDOUT, "request not finished");
     S->by_ticket.erase(it);
-    lk.unlock();  // the request is this caller's now: order and copy its rows outside the lock
-    std::sort(q->rows.begin(), q->rows.end(),
-              [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+    lk.unlock();  // the request is this caller's now: copy its rows outside the lock
     if (rows) *rows = q->rows.size();
     if (latency_ms) *latency_ms = q->latency_ms;
     if (out) std::copy(q->rows.begin(), q->rows.begin() + std::min<uint64_t>(cap, q->rows.size()), out);

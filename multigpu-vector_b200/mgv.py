@@ -552,11 +552,12 @@ class Server:
         return st, t.value
 
     def wait(self, ticket: int, timeout_ms: int = 60000, max_rows: int = 1 << 20):
+        """(status, rows sorted by group, latency_ms); the server returns groups unordered."""
         arr = (GroupRow * max_rows)()
         n = c_uint64()
         lat = c_double()
         st = load().mgv_server_wait(self.h, ticket, timeout_ms, arr, max_rows, byref(n), byref(lat))
-        return st, [(r.group, r.sum, r.count) for r in arr[:min(n.value, max_rows)]], lat.value
+        return st, sorted((r.group, r.sum, r.count) for r in arr[:min(n.value, max_rows)]), lat.value
 
     def stats(self) -> ServerStats:
         st = ServerStats()
