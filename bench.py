@@ -187,6 +187,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 24)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and served summaries added to the join line (N = 1)")
     ap.add_argument("--load-factor", type=float, default=0.5)
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
@@ -323,8 +325,44 @@ def main():
         cpu = {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
                "sample": f"first {sample} probe rows against the full 2^22-key chained table "
                          f"(built once, untimed); {dt:.2f} s on {threads} threads"}
+    # ---- the metric's other half: batched and served queries vs plain (N = 1) ----
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = run_extras(args, mgv, torch, ctx)
     return finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank,
-                  dist, (probe, agg, bhead, hb), nb, npb, tuning)
+                  dist, (probe, agg, bhead, hb), nb, npb, tuning, extras)
+
+
+def run_extras(args, mgv, torch, ctx):
+    """The 512-query batched mix (autotuned) and the served mix, as in
+    `--workload batched` / `--workload served`, summarised for the join line."""
+    import workloads
+
+    class NoClock:
+        def mark(self, *a):
+            pass
+
+    sub = argparse.Namespace(**vars(args))
+    sub.steps, sub.warmup, sub.batch_config = 5, 3, None
+    t0 = time.time()
+    batched = workloads.run_batched(sub, mgv, torch, ctx, None, NoClock(), emit=False)
+    served = workloads.run_served(sub, mgv, torch, ctx, None, NoClock(), emit=False)
+    torch.cuda.empty_cache()
+    at = {r["rate"]: r for r in served["rates"]}
+    return {
+        "batched": {"value": batched["value"], "unit": "queries/s", "ms_per_batch": batched["ms"],
+                    "plain_value": batched["plain"]["value"], "speedup_vs_plain": batched["speedup_vs_plain"],
+                    "workload": batched["workload"], "batch_config": batched["batch_config"],
+                    "checked": batched["checked"]},
+        "served": {"saturated_qps": served["value"], "saturated_plain_qps": served["saturated"]["plain"]["throughput_qps"],
+                   "saturated_speedup_vs_plain": served["saturated_speedup_vs_plain"],
+                   "saturated_detail": served["saturated"],
+                   "p50_p99_ms": {str(r): {"batched": [at[r]["batched"]["p50_ms"], at[r]["batched"]["p99_ms"]],
+                                           "plain": [at[r]["plain"]["p50_ms"], at[r]["plain"]["p99_ms"]]}
+                                  for r in at},
+                   "workload": served["workload"], "checked": served["checked"]},
+        "extras_wall_s": time.time() - t0,
+    }
 
 
 def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, want):
@@ -370,7 +408,7 @@ def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world,
 
 
 def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank, dist,
-           ops, nb, npb, tuning):
+           ops, nb, npb, tuning, extras=None):
     import replicas
 
     value = replicas.job_rate(world, npb * args.steps, elapsed)
@@ -400,6 +438,7 @@ def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, 
         "clocks": clk.summary(),
         "result": {"count": cnt, "sum": s},
     }
+    line.update(extras or {})
     if rank == 0:
         print(json.dumps(line), flush=True)
     for o in ops:

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(kThreads, MB)
     if (warp == kConsumerWarps) {
         // ---- producer warp: keep S tiles of the probe columns in flight ----
         if (lane == 0) {
+            const uint64_t stream_policy = l2_policy_evict_first();  // columns are read once; the table stays
             uint64_t i = 0;
             for (; i < my_tiles; ++i) {
                 const int s = (int)(i % S);
@@ -214,8 +215,8 @@ __global__ void __launch_bounds__(kThreads, MB)
                 }
                 const uint64_t tile = blockIdx.x + i * gridDim.x;
                 mbar_expect_tx(&full[s], ADD_PP ? 2 * tile_bytes : tile_bytes);
-                bulk_g2s(sk + s * T, keys + tile * T, tile_bytes, &full[s]);
-                if (ADD_PP) bulk_g2s(sp + s * T, pays + tile * T, tile_bytes, &full[s]);
+                bulk_g2s_hint(sk + s * T, keys + tile * T, tile_bytes, &full[s], stream_policy);
+                if (ADD_PP) bulk_g2s_hint(sp + s * T, pays + tile * T, tile_bytes, &full[s], stream_policy);
             }
             // let every copy issued land before the CTA can exit
             const uint64_t lo = i > (uint64_t)S ? i - S : 0;

@@ -165,7 +165,8 @@ def _mix(ctx, torch, mgv, nq, seed, stream):
     return spec, descs, (B, P)
 
 
-def run_batched(args, mgv, torch, ctx, bench, clk):
+def run_batched(args, mgv, torch, ctx, bench, clk, emit=True):
+    """Batched vs one-at-a-time queries/s; prints its line when emit, returns its figures."""
     stream = torch.cuda.Stream()
     nq = args.queries
     spec, descs, keep = _mix(ctx, torch, mgv, nq, 0x5EED0004, stream)
@@ -202,21 +203,25 @@ def run_batched(args, mgv, torch, ctx, bench, clk):
     tb, tp = statistics.median(bt), statistics.median(pt)
     rows = sum(x[1] for x in spec)
     st = b.stats()
-    _line(args, "batched queries/s vs plain", nq / tb, "queries/s", 1000 * tb,
-          f"{nq} select->join->group-by queries, build 2^U(10,22), probe 2^U(12,24) rows (total {rows}), "
-          "selectivity U(1%,90%), groups 2^U(4,16); one batch (CUDA graph replay) incl. results to host",
-          {"plain": {"value": nq / tp, "unit": "queries/s", "ms": 1000 * tp,
-                     "how": "the same queries one at a time: hash_build open/consume/close, then "
-                            "select->hash_probe->groupby open/consume/close, operators created once"},
-           "speedup_vs_plain": tp / tb,
-           "batch_config": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
-                            "item_order": cfg.item_order, "autotuned": not args.batch_config, "tune_s": tune_s},
-           "arena_bytes": st.arena_bytes, "probe_rows": rows,
-           "probe_rows_per_s": rows / tb, "checked": "all queries equal between batched and plain"}, clk)
+    workload = (f"{nq} select->join->group-by queries, build 2^U(10,22), probe 2^U(12,24) rows (total {rows}), "
+                "selectivity U(1%,90%), groups 2^U(4,16); one batch (CUDA graph replay) incl. results to host")
+    extra = {"plain": {"value": nq / tp, "unit": "queries/s", "ms": 1000 * tp,
+                       "how": "the same queries one at a time: hash_build open/consume/close, then "
+                              "select->hash_probe->groupby open/consume/close, operators created once"},
+             "speedup_vs_plain": tp / tb,
+             "batch_config": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
+                              "item_order": cfg.item_order, "autotuned": not args.batch_config, "tune_s": tune_s},
+             "arena_bytes": st.arena_bytes, "probe_rows": rows,
+             "probe_rows_per_s": rows / tb, "checked": "all queries equal between batched and plain"}
+    if emit:
+        _line(args, "batched queries/s vs plain", nq / tb, "queries/s", 1000 * tb, workload, extra, clk)
     b.destroy()
+    del keep
+    return {"value": nq / tb, "unit": "queries/s", "ms": 1000 * tb, "workload": workload, **extra}
 
 
-def run_served(args, mgv, torch, ctx, bench, clk):
+def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
+    """Served throughput and p50 / p99 vs the plain server; prints its line when emit, returns its figures."""
     import numpy as np
 
     stream = torch.cuda.Stream()
@@ -320,14 +325,17 @@ def run_served(args, mgv, torch, ctx, bench, clk):
         out.append({"rate": rate if rate else "saturated", "batched": b, "plain": p})
     clk.mark(h0, time.time())
     sat = out[-1]
-    _line(args, "served queries/s & p99 latency vs plain", sat["batched"]["throughput_qps"], "queries/s",
-          sat["batched"]["mean_ms"],
-          "open-loop Poisson arrivals of the batched mix over 16 resident tables (build 2^U(10,22), probe "
-          "2^U(12,24) rows, selectivity U(1%,90%), groups 2^U(4,16)) at each rate, then a burst of "
-          f"{args.saturate} requests (saturated); 40 GB budget; continuous batching",
-          {"rates": out[:-1], "saturated": sat,
-           "saturated_speedup_vs_plain": sat["batched"]["throughput_qps"] / sat["plain"]["throughput_qps"],
-           "checked": "every request's result equals the plain server's"}, clk)
+    workload = ("open-loop Poisson arrivals of the batched mix over 16 resident tables (build 2^U(10,22), probe "
+                "2^U(12,24) rows, selectivity U(1%,90%), groups 2^U(4,16)) at each rate, then a burst of "
+                f"{args.saturate} requests (saturated); 40 GB budget; continuous batching")
+    extra = {"rates": out[:-1], "saturated": sat,
+             "saturated_speedup_vs_plain": sat["batched"]["throughput_qps"] / sat["plain"]["throughput_qps"],
+             "checked": "every request's result equals the plain server's"}
+    if emit:
+        _line(args, "served queries/s & p99 latency vs plain", sat["batched"]["throughput_qps"], "queries/s",
+              sat["batched"]["mean_ms"], workload, extra, clk)
+    del tables
+    return {"value": sat["batched"]["throughput_qps"], "unit": "queries/s", "workload": workload, **extra}
 
 
 def run(args) -> int:
