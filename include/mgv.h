@@ -292,6 +292,20 @@ mgv_status mgv_op_result(mgv_op *op, void *out, size_t bytes, size_t *needed);
 mgv_status mgv_sink_read(mgv_op *sink, uint32_t col, int32_t *dst, uint64_t max_rows,
                          uint64_t *rows);
 
+/* Result delivery channel (replaces gpu_to_cpu's catcher thread and the pool
+ * buffer swap, src/operators/gpu_to_cpu.cu:41-165, src/buffer_manager.cuh:147-176).
+ * Between consume calls of an open sink: waits for `stream`, copies every
+ * row gathered so far (column c to dst_cols[c], c < ncols; host or device
+ * memory, pinned host memory copies fastest) and returns the sink's pool
+ * buffers, so one open sink can deliver any number of rows through a
+ * bounded pool.  Each consume between drains must fit the free buffers of
+ * the pool (otherwise it reports MGV_ENOMEM at the drain).  With dst_cols
+ * NULL only *rows (the rows waiting) is set.  If more rows wait than
+ * cap_rows, nothing is copied or returned and the call fails with
+ * MGV_EINVAL. */
+mgv_status mgv_sink_drain(mgv_op *sink, int32_t *const *dst_cols, uint32_t ncols, uint64_t cap_rows,
+                          uint64_t *rows, void *stream);
+
 /* ---- seeded synthetic columns ------------------------------------------ */
 /*
  * Fill device memory with seeded columns; value i is a pure function of

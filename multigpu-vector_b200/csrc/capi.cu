@@ -767,6 +767,53 @@ mgv_status mgv_sink_read(mgv_op* o, uint32_t col, int32_t* dst, uint64_t max_row
     return MGV_OK;
 }
 
+mgv_status mgv_sink_drain(mgv_op* o, int32_t* const* dst_cols, uint32_t ncols, uint64_t cap_rows, uint64_t* rows,
+                          void* stream) {
+    if (!o || !rows) return fail(MGV_EINVAL, "NULL argument");
+    if (o->kind != OpKind::Sink) return fail(MGV_EINVAL, "not a sink");
+    if (o->state != OpState::Open) return fail(MGV_ESTATE, "sink is not open");
+    if (dst_cols && (ncols == 0 || ncols > o->sink.pool_ncols)) return fail(MGV_EINVAL, "column count out of range");
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    cudaStream_t s = pick_stream(o->ctx, stream);
+    mgv_status st = check_device(o->ctx, s);  // waits for the consumes; a pool that ran dry is reported here
+    if (st != MGV_OK) return st;
+    unsigned long long gathered = 0;
+    std::vector<uint32_t> chain(o->sink.max_chunks);
+    MGV_CUDA_TRY(cudaMemcpyAsync(&gathered, o->sink.cursor, sizeof(gathered), cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(chain.data(), o->sink.chain, sizeof(uint32_t) * chain.size(), cudaMemcpyDeviceToHost,
+                                 s));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+    const uint64_t cap = o->sink.capacity;
+    const uint64_t chunks = (gathered + cap - 1) / cap;
+    std::vector<uint32_t> ids;
+    for (uint64_t c = 0; c < chunks && c < chain.size(); ++c) {
+        if (chain[c] >= o->sink_pool->nbuffers) return fail(MGV_EDEVICE, "sink chunk without a buffer");
+        ids.push_back(chain[c]);
+    }
+    *rows = gathered;
+    if (!dst_cols) return MGV_OK;
+    if (gathered > cap_rows) return fail(MGV_EINVAL, "more rows wait than the destination holds");
+    for (uint32_t col = 0; col < ncols; ++col) {
+        uint64_t done = 0;
+        for (size_t c = 0; c < ids.size(); ++c) {
+            const uint64_t n = std::min<uint64_t>(cap, gathered - done);
+            const int32_t* src = o->sink.slab + ((size_t)ids[c] * o->sink.pool_ncols + col) * cap;
+            MGV_CUDA_TRY(cudaMemcpyAsync(dst_cols[col] + done, src, n * sizeof(int32_t), cudaMemcpyDefault, s));
+            done += n;
+        }
+    }
+    // the sink starts over: buffers back to the pool once the copies are done
+    MGV_CUDA_TRY(cudaMemsetAsync(o->sink.cursor, 0, sizeof(unsigned long long), s));
+    MGV_CUDA_TRY(cudaMemsetAsync(o->sink.chain, 0xff, sizeof(uint32_t) * o->sink.max_chunks, s));
+    MGV_CUDA_TRY(cudaStreamSynchronize(s));
+    if (!ids.empty()) {
+        Pool* p = o->sink_pool;
+        std::lock_guard<std::mutex> lk(p->mu);
+        MGV_CUDA_TRY(pool_push_batch(p, ids.data(), (uint32_t)ids.size()));
+    }
+    return MGV_OK;
+}
+
 // ---- consume: match the chain to a fused kernel ---------------------------
 
 static bool all_open(Op* o) {

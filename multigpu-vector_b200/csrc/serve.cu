@@ -96,6 +96,9 @@ struct mgv_server {
     uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0;
     // plain mode: group-by operators (device tables) reused per max_groups
     std::map<uint32_t, mgv_op*> plain_gb;
+    // Stream-ordered pool for the batches' regions; it keeps freed memory
+    // (no trimming at synchronisations), so a batch does not map fresh pages.
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -156,7 +159,7 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     const size_t ci_off = off;
     off = align256(off + sizeof(BatchItem) * std::max<size_t>(ci.size(), 1));
 
-    MGV_CUDA_TRY(cudaMallocAsync(&sl.dmem, off, sl.stream));
+    MGV_CUDA_TRY(cudaMallocFromPoolAsync(&sl.dmem, off, S->pool, sl.stream));
     unsigned char* A = static_cast<unsigned char*>(sl.dmem);
     // pinned landing zone: rows + counts
     const size_t need_rows = std::max<uint64_t>(rows, 1);
@@ -371,6 +374,20 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
     if (S->cfg.max_inflight > 16) S->cfg.max_inflight = 16;
     if (S->cfg.load_factor == 0.0f) S->cfg.load_factor = ctx->tuning.default_load_factor;
     S->slots.resize(S->cfg.max_inflight);
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        cudaError_t e = cudaMemPoolCreate(&S->pool, &props);
+        uint64_t keep = UINT64_MAX;
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            if (S->pool) cudaMemPoolDestroy(S->pool);
+            delete S;
+            return cuda_fail(e, "mgv_server_create (memory pool)");
+        }
+    }
     for (auto& sl : S->slots) {
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
@@ -495,6 +512,7 @@ mgv_status mgv_server_destroy(mgv_server* S) {
     }
     for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
     for (mgv_op* t : S->tables) mgv_op_destroy(t);
+    if (S->pool) cudaMemPoolDestroy(S->pool);
     delete S;
     return MGV_OK;
 }

@@ -192,6 +192,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_op_close": (st, [c_void_p, c_void_p]),
         "mgv_op_result": (st, [c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]),
         "mgv_sink_read": (st, [c_void_p, c_uint32, c_void_p, c_uint64, POINTER(c_uint64)]),
+        "mgv_sink_drain": (st, [c_void_p, c_void_p, c_uint32, c_uint64, POINTER(c_uint64), c_void_p]),
         "mgv_gen_uniform": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_int64, c_uint64, c_void_p]),
         "mgv_gen_perm": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_void_p]),
         "mgv_gen_probe_keys": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint64, c_uint64, c_uint32,
@@ -464,6 +465,17 @@ class Op:
     def sink_read(self, col: int, dst_ptr: int, max_rows: int) -> int:
         n = c_uint64()
         _call("mgv_sink_read", self.h, col, c_void_p(dst_ptr), max_rows, byref(n))
+        return n.value
+
+    def sink_drain(self, dsts=None, cap_rows: int = 0, stream=None) -> int:
+        """mgv_sink_drain: move the rows gathered so far to dsts (one address or
+        tensor per column) and return the pool buffers; dsts None = only count."""
+        n = c_uint64()
+        if dsts is None:
+            _call("mgv_sink_drain", self.h, None, 0, 0, byref(n), _stream(stream))
+        else:
+            arr = (c_void_p * len(dsts))(*[_ptr(d) for d in dsts])
+            _call("mgv_sink_drain", self.h, arr, len(dsts), cap_rows, byref(n), _stream(stream))
         return n.value
 
     def destroy(self) -> None:
