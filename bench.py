@@ -197,7 +197,7 @@ def main():
     ap.add_argument("--rows-per-thread", type=int, default=None)
     ap.add_argument("--stages", type=int, default=None)
     ap.add_argument("--ctas-per-sm", type=int, default=None)
-    ap.add_argument("--workload", default="join", choices=["join", "select", "pipeline", "batched", "served"],
+    ap.add_argument("--workload", default="join", choices=["join", "select", "pipeline", "batched", "served", "delivery"],
                     help="join: the headline probe; the others are the remaining configurations")
     ap.add_argument("--queries", type=int, default=512, help="batched: queries in the mix")
     ap.add_argument("--batch-config", default=None,

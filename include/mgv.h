@@ -294,15 +294,18 @@ mgv_status mgv_sink_read(mgv_op *sink, uint32_t col, int32_t *dst, uint64_t max_
 
 /* Result delivery channel (replaces gpu_to_cpu's catcher thread and the pool
  * buffer swap, src/operators/gpu_to_cpu.cu:41-165, src/buffer_manager.cuh:147-176).
- * Between consume calls of an open sink: waits for `stream`, copies every
- * row gathered so far (column c to dst_cols[c], c < ncols; host or device
- * memory, pinned host memory copies fastest) and returns the sink's pool
- * buffers, so one open sink can deliver any number of rows through a
- * bounded pool.  Each consume between drains must fit the free buffers of
- * the pool (otherwise it reports MGV_ENOMEM at the drain).  With dst_cols
- * NULL only *rows (the rows waiting) is set.  If more rows wait than
- * cap_rows, nothing is copied or returned and the call fails with
- * MGV_EINVAL. */
+ * Between consume calls of an open sink: waits for `stream`, then starts
+ * copying every row gathered so far (column c to dst_cols[c], c < ncols;
+ * host or device memory, pinned host memory copies fastest) on the sink's
+ * own copy stream and starts the sink over, so the next consume overlaps
+ * the copy and one open sink can deliver any number of rows through a
+ * bounded pool.  The copy is complete, and its buffers are back in the
+ * pool, when the next mgv_sink_drain or mgv_op_close of the sink returns;
+ * read the destination only then.  Each consume between drains must fit
+ * the pool's free buffers (otherwise the drain reports MGV_ENOMEM).  With
+ * dst_cols NULL it only completes the copy in flight and sets *rows to the
+ * rows waiting.  If more rows wait than cap_rows, nothing is copied and the
+ * call fails with MGV_EINVAL. */
 mgv_status mgv_sink_drain(mgv_op *sink, int32_t *const *dst_cols, uint32_t ncols, uint64_t cap_rows,
                           uint64_t *rows, void *stream);
 

@@ -103,6 +103,19 @@ static mgv_status close_groupby(Op* o, cudaStream_t s) {
     return MGV_OK;
 }
 
+// Waits for a sink's copy in flight and returns its buffers to the pool.
+static mgv_status sink_finish_drain(Op* o) {
+    if (!o->drain_done) return MGV_OK;
+    MGV_CUDA_TRY(cudaEventSynchronize(o->drain_done));
+    if (!o->drain_ids.empty()) {
+        Pool* p = o->sink_pool;
+        std::lock_guard<std::mutex> lk(p->mu);
+        MGV_CUDA_TRY(pool_push_batch(p, o->drain_ids.data(), (uint32_t)o->drain_ids.size()));
+        o->drain_ids.clear();
+    }
+    return MGV_OK;
+}
+
 extern "C" {
 
 const char* mgv_status_string(mgv_status s) {
@@ -574,7 +587,12 @@ mgv_status mgv_op_destroy(mgv_op* o) {
     if (!o) return MGV_OK;
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
-    if (o->kind == OpKind::Sink) sink_return_buffers(o);
+    if (o->kind == OpKind::Sink) {
+        sink_finish_drain(o);
+        sink_return_buffers(o);
+        if (o->drain_done) cudaEventDestroy(o->drain_done);
+        if (o->drain_stream) cudaStreamDestroy(o->drain_stream);
+    }
     if (o->h_res) cudaFreeHost(o->h_res);
     if (o->rb_scratch) cudaFree(o->rb_scratch);
     if (o->gb_land) cudaFreeHost(o->gb_land);
@@ -691,6 +709,10 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
     cudaStream_t s = pick_stream(o->ctx, stream);
     o->state = OpState::Closed;
     mgv_status st = MGV_OK;
+    if (o->kind == OpKind::Sink) {  // a drain's copies in flight complete before close returns
+        st = sink_finish_drain(o);
+        if (st != MGV_OK) return st;
+    }
     if (o->kind == OpKind::HashBuild && o->hb_fresh) {  // nothing was built: clear the table now
         MGV_CUDA_TRY(launch_fill_u64(o->table.slots, 4ull * o->table.nbuckets, kEmptySlot, s, o->ctx));
         o->hb_fresh = false;
@@ -775,7 +797,10 @@ mgv_status mgv_sink_drain(mgv_op* o, int32_t* const* dst_cols, uint32_t ncols, u
     if (dst_cols && (ncols == 0 || ncols > o->sink.pool_ncols)) return fail(MGV_EINVAL, "column count out of range");
     MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
     cudaStream_t s = pick_stream(o->ctx, stream);
-    mgv_status st = check_device(o->ctx, s);  // waits for the consumes; a pool that ran dry is reported here
+    // the previous drain's copies complete first: its buffers go back to the pool
+    mgv_status st = sink_finish_drain(o);
+    if (st != MGV_OK) return st;
+    st = check_device(o->ctx, s);  // waits for the consumes; a pool that ran dry is reported here
     if (st != MGV_OK) return st;
     unsigned long long gathered = 0;
     std::vector<uint32_t> chain(o->sink.max_chunks);
@@ -793,24 +818,29 @@ mgv_status mgv_sink_drain(mgv_op* o, int32_t* const* dst_cols, uint32_t ncols, u
     *rows = gathered;
     if (!dst_cols) return MGV_OK;
     if (gathered > cap_rows) return fail(MGV_EINVAL, "more rows wait than the destination holds");
+    if (!o->drain_stream) {
+        MGV_CUDA_TRY(cudaStreamCreateWithFlags(&o->drain_stream, cudaStreamNonBlocking));
+        MGV_CUDA_TRY(cudaEventCreateWithFlags(&o->drain_done, cudaEventDisableTiming));
+    }
+    // The copies run on the sink's own stream, so the next consume on `s`
+    // overlaps them; its buffers stay out of the pool until they are done.
+    MGV_CUDA_TRY(cudaEventRecord(o->drain_done, s));
+    MGV_CUDA_TRY(cudaStreamWaitEvent(o->drain_stream, o->drain_done, 0));
     for (uint32_t col = 0; col < ncols; ++col) {
         uint64_t done = 0;
         for (size_t c = 0; c < ids.size(); ++c) {
             const uint64_t n = std::min<uint64_t>(cap, gathered - done);
             const int32_t* src = o->sink.slab + ((size_t)ids[c] * o->sink.pool_ncols + col) * cap;
-            MGV_CUDA_TRY(cudaMemcpyAsync(dst_cols[col] + done, src, n * sizeof(int32_t), cudaMemcpyDefault, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(dst_cols[col] + done, src, n * sizeof(int32_t), cudaMemcpyDefault,
+                                         o->drain_stream));
             done += n;
         }
     }
-    // the sink starts over: buffers back to the pool once the copies are done
+    MGV_CUDA_TRY(cudaEventRecord(o->drain_done, o->drain_stream));
+    o->drain_ids = ids;
+    // the sink starts over
     MGV_CUDA_TRY(cudaMemsetAsync(o->sink.cursor, 0, sizeof(unsigned long long), s));
     MGV_CUDA_TRY(cudaMemsetAsync(o->sink.chain, 0xff, sizeof(uint32_t) * o->sink.max_chunks, s));
-    MGV_CUDA_TRY(cudaStreamSynchronize(s));
-    if (!ids.empty()) {
-        Pool* p = o->sink_pool;
-        std::lock_guard<std::mutex> lk(p->mu);
-        MGV_CUDA_TRY(pool_push_batch(p, ids.data(), (uint32_t)ids.size()));
-    }
     return MGV_OK;
 }
 

@@ -150,6 +150,11 @@ struct Op {
     SinkView sink{};
     uint64_t sink_rows = 0;
     std::vector<uint32_t> sink_chain;
+    // delivery channel (mgv_sink_drain): copies run on their own stream; the
+    // buffers of the copy in flight return to the pool when it completes
+    cudaStream_t drain_stream = nullptr;
+    cudaEvent_t drain_done = nullptr;
+    std::vector<uint32_t> drain_ids;
     // group-by
     mgv_groupby_desc gb{};
     GroupTableView gtab{};
