@@ -74,11 +74,22 @@ def run_select(args, mgv, torch, ctx, bench, clk):
     cnt, s = agg.result()
     t = statistics.median(times)
     peak, kind = bench.measured_peaks()
+    # CPU baseline: the oracle's restatement of sum_select_cpu (src/main9.cu:56-61), one core, all rows
+    import pyoracle as po
+
+    hc0, hc1 = c0.cpu().numpy(), c1.cpu().numpy()
+    ct = time.perf_counter()
+    for _ in range(5):
+        ref = po.select_agg(hc0, hc1, (1 << 30) - 1)
+    cdt = (time.perf_counter() - ct) / 5
+    assert ref == (cnt, s), (ref, cnt, s)
+    cpu = {"value": n / cdt, "unit": "rows/s", "cores": 1, "kind": "port",
+           "sample": f"all 2^22 rows, mean of 5 runs ({cdt * 1e3:.1f} ms each)"}
     _line(args, "select+aggregate rows/s", n / t, "rows/s", 1000 * t,
           "select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between steps",
           {"roofline": {"bound": "hbm", "achieved": 8 * n / t / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": 8 * n / t / 1e9 / peak, "peak_kind": kind},
-           "result": {"count": cnt, "sum": s},
+           "result": {"count": cnt, "sum": s}, "cpu_baseline": cpu,
            "note": "step = open -> consume -> close incl. the host read-back; 33.5 MB per step"}, clk)
     head.destroy()
     agg.destroy()
@@ -119,6 +130,23 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
     b, p_ = statistics.median(bt), statistics.median(pt)
     peak, kind = bench.measured_peaks()
     alg = 16 * npb + 4 * nb
+    # CPU baseline: the oracle's select -> chained-table join -> group-by on one core; the full
+    # 2^24-key build is timed once, the probe side on a 2^22-row sample, scaled to 2^27 rows
+    import pyoracle as po
+
+    sample = 1 << 22
+    hb_keys = bk.cpu().numpy()
+    hcols = [c[:sample].cpu().numpy() for c in cols]
+    ct = time.perf_counter()
+    po.run_query(hb_keys, hcols[0][:0], hcols[1][:0], hcols[2][:0], hcols[3][:0], 99)
+    t_build = time.perf_counter() - ct
+    ct = time.perf_counter()
+    po.run_query(hb_keys, *hcols, 99)
+    t_probe = time.perf_counter() - ct - t_build
+    cpu_s = t_build + t_probe * npb / sample
+    cpu = {"value": npb / cpu_s, "unit": "rows/s", "cores": 1, "kind": "port",
+           "sample": f"full 2^24-key chained-table build ({t_build:.2f} s) + select/probe/group-by of the "
+                     f"first 2^22 probe rows ({t_probe:.2f} s), scaled to 2^27 rows"}
     _line(args, "select->join->group-by probe rows/s", npb / (b + p_), "rows/s", 1000 * (b + p_),
           "select (filter <= 99 of U[0,1000)) -> join (2^27 probe rows, key over 2^24 build keys) -> group-by "
           "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key bits",
@@ -126,7 +154,7 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
                         "frac": alg / (b + p_) / 1e9 / peak, "peak_kind": kind,
                         "algorithmic_bytes_per_step": alg},
            "phases_ms": {"partition+build": 1000 * b, "select+probe+groupby": 1000 * p_},
-           "result": {"groups": len(res), "count": total}}, clk)
+           "result": {"groups": len(res), "count": total}, "cpu_baseline": cpu}, clk)
     for o in (sel, gb, hb, part):
         o.destroy()
 
@@ -404,6 +432,7 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
 
 def run(args) -> int:
     sys.path.insert(0, HERE)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))  # the CPU baselines time the oracle
     import torch
 
     import bench  # the repo-root benchmark script: peaks and clock sampling
