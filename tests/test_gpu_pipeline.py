@@ -150,3 +150,36 @@ def test_select_probe_aggregate_and_sink(ctx, torch_cuda, dup):
     for x in (sel, pr, agg, sel2, pr2, sink, hb):
         x.destroy()
     pool.destroy()
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3])
+def test_chain_unaligned_columns_and_reserved_keys(ctx, torch_cuda, offset):
+    """select -> join -> group-by over columns that start at different 4-byte
+    offsets, with duplicate build keys and INT32_MIN keys on both sides."""
+    torch = torch_cuda
+    mn = -(1 << 31)
+    nb, npb = 3000, 100003
+    bk = po.gen_uniform(nb, 0x5EED0905, 0, 0, 2000)
+    bk[:7] = mn
+    pk = po.gen_uniform(npb, 0x5EED0905, 1, 0, 2500)
+    pk[::997] = mn
+    pf = po.gen_uniform(npb, 0x5EED0905, 2, 0, 100)
+    pg = po.gen_zipf(npb, 0x5EED0905, 3, 300)
+    pv = po.gen_uniform(npb, 0x5EED0905, 4, -(1 << 31), 1 << 32)
+    hb = mgv.Op.hash_build(ctx, 0, -1, nb)
+    hb.open(); hb.consume_columns([dev(torch, bk)], nb); hb.close()
+    gb = mgv.Op.groupby(ctx, 2, 3, 300)
+    pr = mgv.Op.hash_probe(ctx, 0, hb, gb)
+    sel = mgv.Op.select(ctx, 1, 60, pr)
+    # each column starts at its own 4-byte offset inside a larger allocation
+    cols = []
+    for i, c in enumerate([pk, pf, pg, pv]):
+        o = (offset + i) % 4
+        big = torch.empty(npb + 8, dtype=torch.int32, device="cuda")
+        big[o:o + npb] = torch.from_numpy(c).to("cuda")
+        cols.append(big[o:o + npb])
+    sel.open(); sel.consume_columns(cols, npb); sel.close()
+    want, _, _ = po.run_query(bk, pk, pf, pg, pv, 60)
+    assert gb.result() == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want]
+    for o in (sel, pr, gb, hb):
+        o.destroy()
