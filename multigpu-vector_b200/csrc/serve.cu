@@ -52,7 +52,8 @@ struct Inflight {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     std::vector<std::shared_ptr<Request>> reqs;
-    void* dmem = nullptr;
+    void* dmem = nullptr;    // the slot's device region, kept and grown on demand
+    size_t dmem_cap = 0;
     size_t charge = 0;
     mgv_group_row* h_rows = nullptr;  // pinned
     size_t h_cap = 0;                 // rows
@@ -96,9 +97,6 @@ struct mgv_server {
     uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0;
     // plain mode: group-by operators (device tables) reused per max_groups
     std::map<uint32_t, mgv_op*> plain_gb;
-    // Stream-ordered pool for the batches' regions; it keeps freed memory
-    // (no trimming at synchronisations), so a batch does not map fresh pages.
-    cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -159,7 +157,17 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     const size_t ci_off = off;
     off = align256(off + sizeof(BatchItem) * std::max<size_t>(ci.size(), 1));
 
-    MGV_CUDA_TRY(cudaMallocFromPoolAsync(&sl.dmem, off, S->pool, sl.stream));
+    // Each slot keeps its region and only grows it (the slot's previous batch
+    // has completed): no allocator runs per batch, so slots never wait on
+    // each other's frees.
+    if (off > sl.dmem_cap) {
+        if (sl.dmem) MGV_CUDA_TRY(cudaFree(sl.dmem));
+        sl.dmem = nullptr;
+        sl.dmem_cap = 0;
+        const size_t cap = off + off / 4;
+        MGV_CUDA_TRY(cudaMalloc(&sl.dmem, cap));
+        sl.dmem_cap = cap;
+    }
     unsigned char* A = static_cast<unsigned char*>(sl.dmem);
     // pinned landing zone: rows + counts
     const size_t need_rows = std::max<uint64_t>(rows, 1);
@@ -220,7 +228,6 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
                                  cudaMemcpyDeviceToHost, s));
-    MGV_CUDA_TRY(cudaFreeAsync(sl.dmem, s));
     MGV_CUDA_TRY(cudaEventRecord(sl.done, s));
     sl.busy = true;
     return MGV_OK;
@@ -246,7 +253,6 @@ void finish(mgv_server* S, Inflight& sl) {
     }
     sl.reqs.clear();
     sl.busy = false;
-    sl.dmem = nullptr;
 }
 
 // Plain mode: one request through the operator API (lock not held).
@@ -374,20 +380,6 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
     if (S->cfg.max_inflight > 16) S->cfg.max_inflight = 16;
     if (S->cfg.load_factor == 0.0f) S->cfg.load_factor = ctx->tuning.default_load_factor;
     S->slots.resize(S->cfg.max_inflight);
-    {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = ctx->device;
-        cudaError_t e = cudaMemPoolCreate(&S->pool, &props);
-        uint64_t keep = UINT64_MAX;
-        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        if (e != cudaSuccess) {
-            if (S->pool) cudaMemPoolDestroy(S->pool);
-            delete S;
-            return cuda_fail(e, "mgv_server_create (memory pool)");
-        }
-    }
     for (auto& sl : S->slots) {
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
@@ -507,12 +499,12 @@ mgv_status mgv_server_destroy(mgv_server* S) {
     for (auto& sl : S->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         if (sl.h_rows) cudaFreeHost(sl.h_rows);
+        if (sl.dmem) cudaFree(sl.dmem);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
     for (mgv_op* t : S->tables) mgv_op_destroy(t);
-    if (S->pool) cudaMemPoolDestroy(S->pool);
     delete S;
     return MGV_OK;
 }
