@@ -6,7 +6,7 @@
 // consume makes two passes over its input:
 //   1. k_part_hist: per-CTA shared histograms of (key >> shift) & mask,
 //      merged with one global atomic per partition and CTA;
-//   2. k_part_scatter: tiles of 1024 rows get a local rank per row from a
+//   2. k_part_scatter: tiles of 4096 rows get a local rank per row from a
 //      shared-memory histogram, reserve one contiguous range per partition
 //      from the global cursors (host-initialised to the exclusive prefix sum),
 //      and write every column of the row to its place.
@@ -67,26 +67,40 @@ __global__ void __launch_bounds__(kPartBlock, 2)
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock) cnt[p] = 0;
         __syncthreads();
+        int32_t key[kPartRows];
         uint32_t part[kPartRows], rank[kPartRows];
         bool keep[kPartRows];
+        // every load of the tile first, then the ranks
 #pragma unroll
         for (int r = 0; r < kPartRows; ++r) {
             const uint64_t i = tile * kTile + (uint64_t)r * kPartBlock + threadIdx.x;
             keep[r] = i < n;
+            key[r] = keep[r] ? __ldg(in.cols[key_col] + i) : 0;
             if (SEL && keep[r]) keep[r] = __ldg(filt + i) <= bound;
-            part[r] = keep[r] ? (((uint32_t)__ldg(in.cols[key_col] + i) >> shift) & mask) : 0u;
+        }
+#pragma unroll
+        for (int r = 0; r < kPartRows; ++r) {
+            part[r] = ((uint32_t)key[r] >> shift) & mask;
             rank[r] = keep[r] ? atomicAdd(&cnt[part[r]], 1u) : 0u;
         }
         __syncthreads();
         for (uint32_t p = threadIdx.x; p <= mask; p += kPartBlock)
             shb[p] = cnt[p] ? atomicAdd(cursors + p, (unsigned long long)cnt[p]) : 0ull;
         __syncthreads();
+        uint64_t dst[kPartRows];
 #pragma unroll
-        for (int r = 0; r < kPartRows; ++r) {
-            if (!keep[r]) continue;
-            const uint64_t i = tile * kTile + (uint64_t)r * kPartBlock + threadIdx.x;
-            const uint64_t dst = shb[part[r]] + rank[r];
-            for (uint32_t c = 0; c < ncols; ++c) out[(uint64_t)c * out_stride + dst] = __ldg(in.cols[c] + i);
+        for (int r = 0; r < kPartRows; ++r) dst[r] = keep[r] ? shb[part[r]] + rank[r] : 0ull;
+        // column by column: the tile's loads of a column, then its stores (the key column is in registers)
+        for (uint32_t c = 0; c < ncols; ++c) {
+            int32_t v[kPartRows];
+#pragma unroll
+            for (int r = 0; r < kPartRows; ++r) {
+                const uint64_t i = tile * kTile + (uint64_t)r * kPartBlock + threadIdx.x;
+                v[r] = c == key_col ? key[r] : (keep[r] ? __ldg(in.cols[c] + i) : 0);
+            }
+#pragma unroll
+            for (int r = 0; r < kPartRows; ++r)
+                if (keep[r]) out[(uint64_t)c * out_stride + dst[r]] = v[r];
         }
         __syncthreads();
     }
