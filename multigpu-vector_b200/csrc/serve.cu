@@ -10,7 +10,9 @@
 // requests that arrive while others run are admitted as soon as a stream
 // and memory free up and their work overlaps on the device.  Completion is
 // observed through CUDA events; latency runs from submit to the moment the
-// scheduler sees the batch's results on the host.
+// scheduler sees the batch's results on the host.  The results stay in the
+// batch's pinned landing zone until each waiter copies its own rows out, so
+// the scheduler thread copies nothing and is free to launch the next batch.
 //
 // With plain = 1 the server instead runs requests one at a time through the
 // operator API (select -> hash_probe -> groupby on the resident table): the
@@ -36,6 +38,18 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
+// A pinned host buffer that one batch's results are copied into.  Its rows
+// stay there until every request of the batch has been waited for (the
+// waiter copies its own rows out), then the buffer serves another batch.
+struct Landing {
+    mgv_group_row* rows = nullptr;  // pinned: cap rows, then the per-request counts
+    uint32_t* counts = nullptr;
+    size_t cap = 0;                 // rows
+    uint32_t ncounts = 0;
+    int refs = 0;                   // requests whose rows are here and not yet waited for (lock held)
+    bool attached = false;          // a slot is filling it
+};
+
 struct Request {
     uint64_t ticket = 0;
     mgv_server_request r{};
@@ -44,7 +58,10 @@ struct Request {
     double latency_ms = 0.0;
     mgv_status status = MGV_OK;
     bool done = false;
-    std::vector<mgv_group_row> rows;
+    std::vector<mgv_group_row> rows;  // plain mode
+    Landing* land = nullptr;          // batched mode: the rows are land->rows[off, off + n)
+    uint64_t off = 0;
+    uint32_t n = 0;
     size_t bytes = 0;  // admission charge
 };
 
@@ -55,9 +72,7 @@ struct Inflight {
     void* dmem = nullptr;    // the slot's device region, kept and grown on demand
     size_t dmem_cap = 0;
     size_t charge = 0;
-    mgv_group_row* h_rows = nullptr;  // pinned
-    size_t h_cap = 0;                 // rows
-    uint32_t* h_counts = nullptr;     // pinned, inside h_rows allocation
+    Landing* land = nullptr;          // where this batch's results land
     std::vector<uint64_t> offs;
     bool busy = false;
 };
@@ -97,6 +112,7 @@ struct mgv_server {
     uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0;
     // plain mode: group-by operators (device tables) reused per max_groups
     std::map<uint32_t, mgv_op*> plain_gb;
+    std::vector<std::unique_ptr<Landing>> landings;  // pinned result buffers (lock held)
 };
 
 namespace {
@@ -107,6 +123,36 @@ void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
     q->done = true;
     S->latencies.push_back(q->latency_ms);
     S->completed++;
+}
+
+// A free landing zone of at least `rows` rows and `ncounts` counts (scheduler
+// thread, lock not held; the list is read and changed under the lock, a new
+// zone is pinned outside it).
+mgv_status acquire_landing(mgv_server* S, uint64_t rows, uint32_t ncounts, Landing*& out) {
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        Landing* best = nullptr;
+        for (auto& L : S->landings)
+            if (!L->attached && L->refs == 0 && L->cap >= rows && L->ncounts >= ncounts && (!best || L->cap < best->cap))
+                best = L.get();
+        if (best) {
+            best->attached = true;
+            out = best;
+            return MGV_OK;
+        }
+    }
+    auto L = std::make_unique<Landing>();
+    L->cap = rows + rows / 4;
+    L->ncounts = std::max<uint32_t>(ncounts, S->cfg.max_batch);
+    void* p = nullptr;
+    MGV_CUDA_TRY(cudaMallocHost(&p, sizeof(mgv_group_row) * L->cap + 4ull * L->ncounts));
+    L->rows = static_cast<mgv_group_row*>(p);
+    L->counts = reinterpret_cast<uint32_t*>(L->rows + L->cap);
+    L->attached = true;
+    out = L.get();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->landings.push_back(std::move(L));
+    return MGV_OK;
 }
 
 // Launch one batch of admitted requests on slot `sl` (scheduler thread, lock
@@ -169,14 +215,9 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
         sl.dmem_cap = cap;
     }
     unsigned char* A = static_cast<unsigned char*>(sl.dmem);
-    // pinned landing zone: rows + counts
-    const size_t need_rows = std::max<uint64_t>(rows, 1);
-    if (sl.h_cap < need_rows || !sl.h_rows) {
-        if (sl.h_rows) cudaFreeHost(sl.h_rows);
-        sl.h_cap = std::max<size_t>(need_rows, 2 * sl.h_cap);
-        MGV_CUDA_TRY(cudaMallocHost(&sl.h_rows, sizeof(mgv_group_row) * sl.h_cap + 4ull * (S->cfg.max_batch + 4)));
-        sl.h_counts = reinterpret_cast<uint32_t*>(sl.h_rows + sl.h_cap);
-    }
+    // a pinned landing zone for the results (rows + counts)
+    mgv_status lst = acquire_landing(S, std::max<uint64_t>(rows, 1), nq, sl.land);
+    if (lst != MGV_OK) return lst;
     std::vector<ChainDev> hq(nq);
     std::vector<BatchOut> ho(nq);
     for (uint32_t i = 0; i < nq; ++i) {
@@ -225,32 +266,30 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), reinterpret_cast<BatchOut*>(A + outs_off),
                               reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(),
                               reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, 0u, s, ctx));
-    MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
-    MGV_CUDA_TRY(cudaMemcpyAsync(sl.h_rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
+    MGV_CUDA_TRY(cudaMemcpyAsync(sl.land->counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
+    MGV_CUDA_TRY(cudaMemcpyAsync(sl.land->rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
                                  cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaEventRecord(sl.done, s));
     sl.busy = true;
     return MGV_OK;
 }
 
-// Copies a finished batch's rows out of the slot's pinned buffer into its
-// requests (scheduler thread, lock not held: nothing else touches the slot,
-// and waiters read a request's rows only after complete() under the lock).
-void collect(Inflight& sl) {
-    for (size_t i = 0; i < sl.reqs.size(); ++i) {
-        auto& q = sl.reqs[i];
-        const uint32_t n = std::min<uint32_t>(sl.h_counts[i], q->r.max_groups);
-        q->rows.assign(sl.h_rows + sl.offs[i], sl.h_rows + sl.offs[i] + n);
-    }
-}
-
-// Completes a collected batch (lock held).
+// Hands a finished batch's results to its requests (lock held): each
+// request points at its rows in the batch's landing zone, which stays out of
+// use until every request has been waited for; the slot takes a new one.
 void finish(mgv_server* S, Inflight& sl) {
+    Landing* L = sl.land;
+    L->attached = false;
+    L->refs = (int)sl.reqs.size();
     for (size_t i = 0; i < sl.reqs.size(); ++i) {
         auto& q = sl.reqs[i];
-        complete(S, q, sl.h_counts[i] > q->r.max_groups ? MGV_ENOMEM : MGV_OK);
+        q->land = L;
+        q->off = sl.offs[i];
+        q->n = std::min<uint32_t>(L->counts[i], q->r.max_groups);
+        complete(S, q, L->counts[i] > q->r.max_groups ? MGV_ENOMEM : MGV_OK);
         S->used -= q->bytes;
     }
+    sl.land = nullptr;
     sl.reqs.clear();
     sl.busy = false;
 }
@@ -309,9 +348,6 @@ void scheduler(mgv_server* S) {
         bool any_busy = false;
         for (auto& sl : S->slots) {
             if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) {
-                lk.unlock();
-                collect(sl);
-                lk.lock();
                 finish(S, sl);
                 S->done_cv.notify_all();
             }
@@ -350,6 +386,10 @@ void scheduler(mgv_server* S) {
                     for (auto& q : free_slot->reqs) { S->used -= q->bytes; complete(S, q, st); }
                     free_slot->reqs.clear();
                     free_slot->busy = false;
+                    if (free_slot->land) {  // nothing landed: the zone is free again
+                        free_slot->land->attached = false;
+                        free_slot->land = nullptr;
+                    }
                     S->done_cv.notify_all();
                 }
                 continue;
@@ -446,9 +486,16 @@ mgv_status mgv_server_wait(mgv_server* S, uint64_t ticket, uint32_t timeout_ms, 
         return fail(MGV_ETIMEDOUT, "request not finished");
     S->by_ticket.erase(it);
     lk.unlock();  // the request is this caller's now: copy its rows outside the lock
-    if (rows) *rows = q->rows.size();
+    const mgv_group_row* src = q->land ? q->land->rows + q->off : q->rows.data();
+    const uint64_t n = q->land ? q->n : q->rows.size();
+    if (rows) *rows = n;
     if (latency_ms) *latency_ms = q->latency_ms;
-    if (out) std::copy(q->rows.begin(), q->rows.begin() + std::min<uint64_t>(cap, q->rows.size()), out);
+    if (out) std::copy(src, src + std::min<uint64_t>(cap, n), out);
+    if (q->land) {  // the landing zone is free again once its last request is waited for
+        lk.lock();
+        q->land->refs--;
+        q->land = nullptr;
+    }
     if (q->status != MGV_OK) return fail(q->status, "request failed");
     return MGV_OK;
 }
@@ -498,13 +545,13 @@ mgv_status mgv_server_destroy(mgv_server* S) {
     cudaSetDevice(S->ctx->device);
     for (auto& sl : S->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
-        if (sl.h_rows) cudaFreeHost(sl.h_rows);
         if (sl.dmem) cudaFree(sl.dmem);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
     for (mgv_op* t : S->tables) mgv_op_destroy(t);
+    for (auto& L : S->landings) cudaFreeHost(L->rows);
     delete S;
     return MGV_OK;
 }
