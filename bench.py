@@ -349,6 +349,8 @@ def run_extras(args, mgv, torch, ctx):
     batched = workloads.run_batched(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     served = workloads.run_served(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     torch.cuda.empty_cache()
+    delivery = workloads.run_delivery(sub, mgv, torch, ctx, None, NoClock(), emit=False)
+    torch.cuda.empty_cache()
     at = {r["rate"]: r for r in served["rates"]}
     return {
         "batched": {"value": batched["value"], "unit": "queries/s", "ms_per_batch": batched["ms"],
@@ -362,6 +364,8 @@ def run_extras(args, mgv, torch, ctx):
                                            "plain": [at[r]["plain"]["p50_ms"], at[r]["plain"]["p99_ms"]]}
                                   for r in at},
                    "workload": served["workload"], "checked": served["checked"]},
+        "delivery": {"value": delivery["value"], "unit": "rows/s", "host_gbs": delivery["host_gbs"],
+                     "workload": delivery["workload"]},
         "extras_wall_s": time.time() - t0,
     }
 
