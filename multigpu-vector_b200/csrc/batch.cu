@@ -107,7 +107,7 @@ mgv_status enqueue_run(mgv_batch* b, cudaStream_t s) {
     MGV_CUDA_TRY(cudaMemsetAsync(b->out_counts, 0, sizeof(uint32_t) * b->q.size(), s));
     // every region of every table is written by the build (no clearing pass)
     MGV_CUDA_TRY(launch_build_regions(b->d_jobs, RegionJob{}, (uint32_t)b->q.size(), b->d_build_items, b->n_build, 0, 0,
-                                      b->total_regions, b->max_job_regions, b->rsc, true, s, ctx));
+                                      b->total_regions, b->max_job_regions, b->rsc, true, false, s, ctx));
     MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_outs, b->d_probe_items, b->n_probe, b->d_compact_items, b->n_compact,
                               (int)b->cfg.probe_ctas_per_sm, b->cfg.item_order, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->out_counts, sizeof(uint32_t) * b->q.size(), cudaMemcpyDeviceToHost, s));
@@ -128,9 +128,7 @@ mgv_status check_run(mgv_batch* b) {
     return fail(MGV_EDEVICE, "batch: device error " + std::to_string(code));
 }
 
-void sort_rows(std::vector<mgv_group_row>& v) {
-    std::sort(v.begin(), v.end(), [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
-}
+void sort_rows(std::vector<mgv_group_row>& v) { sort_group_rows(v); }
 
 }  // namespace
 

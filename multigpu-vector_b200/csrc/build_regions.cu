@@ -11,9 +11,11 @@
 //                        range (per item: one global reservation per region,
 //                        then shared-memory cursors)
 //   4. k_region_build    one CTA per region: the region is loaded into shared
-//                        memory (or starts empty), its rows are inserted with
-//                        shared-memory CAS and linear probing, and it is
-//                        written back with coalesced stores
+//                        memory (or starts empty), each row claims a slot
+//                        with one shared atomicAdd on its bucket's fill
+//                        counter (linear probing on a full bucket), a
+//                        conflict-free pass finds duplicate keys, and the
+//                        region is written back with one bulk copy
 //   5. k_region_overflow rows whose run leaves their region (rare) are
 //                        inserted into the finished global table
 // The table is the same open-addressing table (hash_table.cuh): a row goes to
@@ -32,7 +34,7 @@ namespace mgv {
 namespace {
 
 constexpr int kRBlock = 512;      // histogram / scatter CTA
-constexpr int kRBuildBlock = 256; // region build CTA
+constexpr int kRBuildBlock = 512; // region build CTA
 constexpr int kScanBlock = 1024;
 
 // The job of item / region lookups, cached in shared memory by the caller.
@@ -59,8 +61,10 @@ __device__ __forceinline__ uint32_t region_of(int32_t key, const TableView& t) {
 // Loads of kPrefetch rows per thread are issued before any is used.
 constexpr int kPrefetch = 8;
 
-// Adds the item's rows to the shared per-region counters.
-__device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchItem& item, uint32_t* sh) {
+// Adds the item's rows to the shared per-region counters; lo / hi take the
+// smallest and largest region this thread saw.
+__device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchItem& item, uint32_t* sh,
+                                              uint32_t& lo, uint32_t& hi) {
     for (uint64_t i0 = item.lo + threadIdx.x; i0 < item.hi; i0 += (uint64_t)kRBlock * kPrefetch) {
         int32_t key[kPrefetch];
         bool in[kPrefetch];
@@ -73,7 +77,12 @@ __device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchIt
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u)
-            if (in[u] && key[u] != kEmptyKey) atomicAdd(sh + region_of(key[u], sj.t), 1u);
+            if (in[u] && key[u] != kEmptyKey) {
+                const uint32_t r = region_of(key[u], sj.t);
+                atomicAdd(sh + r, 1u);
+                lo = min(lo, r);
+                hi = max(hi, r);
+            }
     }
 }
 
@@ -93,7 +102,8 @@ __global__ void __launch_bounds__(kRBlock) k_region_hist(const RegionJob* __rest
         }
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) sh[r] = 0;
         __syncthreads();
-        count_regions(sj, item, sh);
+        uint32_t lo = ~0u, hi = 0;
+        count_regions(sj, item, sh, lo, hi);
         __syncthreads();
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock)
             if (sh[r]) atomicAdd(hist + sj.region0 + r, sh[r]);
@@ -142,7 +152,8 @@ __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __r
         }
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) sh[r] = 0;
         __syncthreads();
-        count_regions(sj, item, sh);
+        uint32_t lo = ~0u, hi = 0;
+        count_regions(sj, item, sh, lo, hi);
         __syncthreads();
         // one reservation per region and item; sh[r] becomes the region's next staging row
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) {
@@ -176,6 +187,125 @@ __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __r
     }
 }
 
+constexpr int kWarpTileRows = 8;                          // rows per lane of a warp tile
+constexpr uint32_t kWarpTile = 32u * kWarpTileRows;       // 256 rows
+constexpr uint32_t kWarpSpan = 64;                        // widest region span a warp tile sorts
+
+// One warp's sorting space in k_region_scatter_sorted.
+struct WarpSort {
+    unsigned long long val[kWarpTile];  // the tile's rows in region order
+    uint32_t off[kWarpSpan];            // counts, then each region's first sorted position
+    uint32_t base[kWarpSpan];           // staging row of sorted position 0 of each region (mod 2^32)
+    uint8_t reg[kWarpTile];             // region (minus the tile's lowest) of each sorted position
+};
+
+// Rows of input that is already partitioned on the table's radix bits (a
+// partition op's run: each partition's rows together, so a warp's tile of 256
+// rows falls in the regions of one or two partitions).  Each warp sorts its
+// tile by region in its own shared memory -- ranks by shared atomics, one
+// global cursor reservation per region -- and stores runs of consecutive
+// staging rows, with no block-wide barrier.  A tile whose regions span more
+// than kWarpSpan takes one cursor increment per row instead.
+__global__ void __launch_bounds__(kRBlock, 2) k_region_scatter_sorted(RegionJob job, uint64_t n,
+                                                                    uint32_t* __restrict__ cursor,
+                                                                    unsigned long long* __restrict__ staging,
+                                                                    uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char ws_raw[];
+    WarpSort& ws = reinterpret_cast<WarpSort*>(ws_raw)[threadIdx.x / 32];
+    const uint32_t lane = lane_id();
+    const uint64_t ntiles = (n + kWarpTile - 1) / kWarpTile;
+    const uint64_t nw = (uint64_t)gridDim.x * (kRBlock / 32);
+    for (uint64_t tile = (uint64_t)blockIdx.x * (kRBlock / 32) + threadIdx.x / 32; tile < ntiles; tile += nw) {
+        const uint64_t t0 = tile * kWarpTile;
+        int32_t key[kWarpTileRows], pay[kWarpTileRows];
+        bool in[kWarpTileRows];
+#pragma unroll
+        for (int u = 0; u < kWarpTileRows; ++u) {
+            const uint64_t i = t0 + 32u * u + lane;
+            in[u] = i < n;
+            key[u] = in[u] ? __ldg(job.keys + i) : 0;
+            pay[u] = (in[u] && job.pays) ? __ldg(job.pays + i) : 0;
+            if (in[u] && job.filt) in[u] = __ldg(job.filt + i) <= job.bound;
+        }
+        uint32_t reg[kWarpTileRows];
+        uint32_t lo = ~0u, hi = 0;
+#pragma unroll
+        for (int u = 0; u < kWarpTileRows; ++u) {
+            reg[u] = 0;
+            if (!in[u]) continue;
+            if (key[u] == kEmptyKey) {  // the side list (its duplicates are seen from its count)
+                bool dup, ok;
+                table_insert(job.t, key[u], pay[u], err, dup, ok);
+                in[u] = false;
+                continue;
+            }
+            reg[u] = region_of(key[u], job.t);
+            lo = min(lo, reg[u]);
+            hi = max(hi, reg[u]);
+        }
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        if (lo > hi) continue;  // no row of the tile goes to the table
+        if (hi - lo >= kWarpSpan) {
+#pragma unroll
+            for (int u = 0; u < kWarpTileRows; ++u)
+                if (in[u]) {
+                    const uint32_t pos = atomicAdd(cursor + job.region0 + reg[u], 1u);
+                    staging[pos] = ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u];
+                }
+            continue;
+        }
+        const uint32_t span = hi - lo + 1;
+        for (uint32_t j = lane; j < span; j += 32) ws.off[j] = 0;
+        __syncwarp();
+        uint32_t rank[kWarpTileRows];
+#pragma unroll
+        for (int u = 0; u < kWarpTileRows; ++u) {
+            reg[u] -= lo;
+            rank[u] = in[u] ? atomicAdd(&ws.off[reg[u]], 1u) : 0u;
+        }
+        __syncwarp();
+        // lane l owns regions l and l + 32: reserve their staging ranges, then
+        // an exclusive scan of the counts gives their first sorted positions
+        const uint32_t c0 = lane < span ? ws.off[lane] : 0u;
+        const uint32_t c1 = lane + 32 < span ? ws.off[lane + 32] : 0u;
+        const uint32_t g0 = c0 ? atomicAdd(cursor + job.region0 + lo + lane, c0) : 0u;
+        const uint32_t g1 = c1 ? atomicAdd(cursor + job.region0 + lo + lane + 32, c1) : 0u;
+        uint32_t x0 = c0, x1 = c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y0 = __shfl_up_sync(0xffffffffu, x0, o);
+            const uint32_t y1 = __shfl_up_sync(0xffffffffu, x1, o);
+            if (lane >= (uint32_t)o) {
+                x0 += y0;
+                x1 += y1;
+            }
+        }
+        const uint32_t tot0 = __shfl_sync(0xffffffffu, x0, 31);
+        const uint32_t total = tot0 + __shfl_sync(0xffffffffu, x1, 31);
+        const uint32_t e0 = x0 - c0, e1 = tot0 + x1 - c1;
+        if (lane < span) {
+            ws.off[lane] = e0;
+            ws.base[lane] = g0 - e0;
+        }
+        if (lane + 32 < span) {
+            ws.off[lane + 32] = e1;
+            ws.base[lane + 32] = g1 - e1;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < kWarpTileRows; ++u)
+            if (in[u]) {
+                const uint32_t p = ws.off[reg[u]] + rank[u];
+                ws.val[p] = ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u];
+                ws.reg[p] = (uint8_t)reg[u];
+            }
+        __syncwarp();
+        for (uint32_t j = lane; j < total; j += 32) staging[ws.base[ws.reg[j]] + j] = ws.val[j];
+        __syncwarp();  // the warp's buffers are free for its next tile
+    }
+}
+
 __device__ __forceinline__ uint32_t job_of_region(const RegionJob* jobs, uint32_t njobs, uint32_t g) {
     uint32_t lo = 0, hi = njobs;  // last job whose region0 <= g
     while (hi - lo > 1) {
@@ -186,7 +316,7 @@ __device__ __forceinline__ uint32_t job_of_region(const RegionJob* jobs, uint32_
     return lo;
 }
 
-// 16-byte shared-memory read, issued where it stands (not cached across CAS).
+// 16-byte shared-memory read.
 __device__ __forceinline__ uint4 lds_v4(const void* p) {
     uint4 r;
     asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
@@ -196,41 +326,94 @@ __device__ __forceinline__ uint4 lds_v4(const void* p) {
     return r;
 }
 
-// Inserts one staged row into the shared region (linear probing inside it).
-// A slot is claimed with a 32-bit CAS on its key word, then its payload word
-// is stored: nothing reads payloads before the region is written back.
-__device__ __forceinline__ bool region_insert(unsigned long long* tab, uint32_t nb, uint32_t b,
-                                              unsigned long long v, bool& dup) {
-    const uint32_t key = (uint32_t)v;
-    uint32_t* words = reinterpret_cast<uint32_t*>(tab);  // slot q of bucket b: words[8b + 2q] key, +1 payload
+// The four key words of shared bucket b.
+__device__ __forceinline__ void bucket_keys(const unsigned long long* tab, uint32_t b, uint32_t (&k)[4]) {
+    const uint32_t* words = reinterpret_cast<const uint32_t*>(tab) + 8 * b;
+    const uint4 s01 = lds_v4(words), s23 = lds_v4(words + 4);
+    k[0] = s01.x;
+    k[1] = s01.z;
+    k[2] = s23.x;
+    k[3] = s23.z;
+}
+
+// Inserts one staged row into the shared region.  fill[b] counts the rows
+// that asked bucket b for a slot: the first four get slots 0..3 in that order
+// (so slots fill as a prefix, as the global insert leaves them), later ones
+// move on to the next bucket.  A bucket that has turned a row away stays full,
+// so every row ends in the first bucket of its run that had room.
+__device__ __forceinline__ bool region_insert(unsigned long long* tab, uint32_t* fill, uint32_t nb, uint32_t b,
+                                              unsigned long long v) {
     for (; b < nb; ++b) {
-        // the whole bucket in two 16-byte reads; a stale empty key only costs a failed CAS
-        const uint4 s01 = lds_v4(words + 8 * b);
-        const uint4 s23 = lds_v4(words + 8 * b + 4);
-        const uint32_t ks[4] = {s01.x, s01.z, s23.x, s23.z};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t c = ks[q];
-            if (c == (uint32_t)kEmptyKey) {
-                c = atomicCAS(words + 8 * b + 2 * q, (uint32_t)kEmptyKey, key);
-                if (c == (uint32_t)kEmptyKey) {
-                    words[8 * b + 2 * q + 1] = (uint32_t)(v >> 32);
-                    return true;
-                }
-            }
-            if (c == key) dup = true;
+        const uint32_t q = atomicAdd(fill + b, 1u);
+        if (q < 4) {
+            tab[4 * b + q] = v;
+            return true;
         }
     }
     return false;  // the run leaves the region
 }
 
-__global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* __restrict__ jobs, RegionJob job0,
-                                                               uint32_t njobs, uint32_t regions,
-                                                               const uint32_t* __restrict__ start,
-                                                               const unsigned long long* __restrict__ staging,
-                                                               unsigned long long* __restrict__ ovf,
-                                                               uint32_t* ovf_count, uint32_t fresh, uint32_t* err) {
-    extern __shared__ __align__(128) unsigned long long tab[];  // kRegionBuckets * 4 slots
+// Whether bucket b holds a key that also appears later in its run: in b
+// itself, or in the buckets after b up to the first one that is not full.
+// Two rows with one key share their home bucket, and every bucket between
+// the two is full, so this finds every duplicate pair inside the region.
+__device__ __forceinline__ bool bucket_has_dup(const unsigned long long* tab, const uint32_t* fill, uint32_t nb,
+                                               uint32_t b) {
+    const uint32_t n = min(fill[b], 4u);
+    if (n < 2) return false;  // no pair in b, and b is not full
+    uint32_t k[4];
+    bucket_keys(tab, b, k);
+    bool dup = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = i + 1; j < 4; ++j) dup |= (uint32_t)j < n && k[i] == k[j];
+    if (n < 4) return dup;
+    for (uint32_t c = b + 1; c < nb && !dup; ++c) {
+        const uint32_t m = min(fill[c], 4u);
+        uint32_t o[4];
+        bucket_keys(tab, c, o);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dup |= (uint32_t)j < m && k[i] == o[j];
+        if (m < 4) break;
+    }
+    return dup;
+}
+
+constexpr int kBuildRows = 8;  // staging rows per thread in one load batch (4096 per region)
+
+// The next region of this CTA at or after g (stride gridDim.x); without
+// `fresh`, regions that receive no rows are left as they are.
+__device__ __forceinline__ uint32_t next_region(uint32_t g, uint32_t regions, const uint32_t* start, uint32_t fresh) {
+    for (; g < regions; g += gridDim.x)
+        if (fresh || start[g] != start[g + 1]) return g;
+    return regions;
+}
+
+// Staging rows [s0, s1) of a region, the first kBuildRows * kRBuildBlock of
+// them, into registers (rows past s1 read as empty).
+__device__ __forceinline__ void load_region_rows(const unsigned long long* staging, uint32_t s0, uint32_t s1,
+                                                 unsigned long long (&v)[kBuildRows]) {
+#pragma unroll
+    for (int u = 0; u < kBuildRows; ++u) {
+        const uint32_t i = s0 + threadIdx.x + u * kRBuildBlock;
+        v[u] = i < s1 ? staging[i] : kEmptySlot;
+    }
+}
+
+// Regions one at a time per CTA, several CTAs per SM; the next region's
+// first rows are loaded into registers before this region's duplicate pass
+// and bulk store, so their latency overlaps that work.
+__global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJob* __restrict__ jobs, RegionJob job0,
+                                                                  uint32_t njobs, uint32_t regions,
+                                                                  const uint32_t* __restrict__ start,
+                                                                  const unsigned long long* __restrict__ staging,
+                                                                  unsigned long long* __restrict__ ovf,
+                                                                  uint32_t* ovf_count, uint32_t fresh, uint32_t* err) {
+    extern __shared__ __align__(128) unsigned long long tab[];  // kRegionBuckets * 4 slots, then the fill counters
+    uint32_t* fill = reinterpret_cast<uint32_t*>(tab + 4 * kRegionBuckets);
     __shared__ RegionJob sj;
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x == 0) {
@@ -239,9 +422,11 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
     }
     uint32_t phase = 0;
     int64_t cur = -1;
-    for (uint32_t g = blockIdx.x; g < regions; g += gridDim.x) {
+    uint32_t g = next_region(blockIdx.x, regions, start, fresh);
+    unsigned long long v[kBuildRows];
+    if (g < regions) load_region_rows(staging, start[g], start[g + 1], v);
+    while (g < regions) {
         const uint32_t s0 = start[g], s1 = start[g + 1];
-        if (!fresh && s0 == s1) continue;  // nothing to add, the region stays as it is
         const uint32_t j = (jobs && njobs > 1) ? job_of_region(jobs, njobs, g) : 0u;
         __syncthreads();  // the previous region's store has read the buffer; sj is free
         if ((int64_t)j != cur) {
@@ -256,6 +441,7 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
             const uint4 empty = make_uint4(0x80000000u, 0x80000000u, 0x80000000u, 0x80000000u);  // 2 x kEmptySlot
             static_assert(kEmptySlot == 0x8000000080000000ull, "empty slot pattern");
             for (uint32_t w = threadIdx.x; w < 2 * nb; w += kRBuildBlock) reinterpret_cast<uint4*>(tab)[w] = empty;
+            for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) fill[b] = 0;
         } else {
             if (threadIdx.x == 0) {  // the region's current contents, one bulk copy
                 mbar_expect_tx(&bar, nb * 32);
@@ -269,26 +455,35 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
                 return;
             }
             phase ^= 1u;
+            // slots fill as a prefix: a bucket's count is the index of its first empty slot
+            for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) {
+                uint32_t k[4];
+                bucket_keys(tab, b, k);
+                uint32_t n = 0;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) n += k[q] != (uint32_t)kEmptyKey;
+                fill[b] = n;
+            }
         }
         __syncthreads();
         uint32_t ins = 0;
-        bool dup = false;
-        for (uint32_t i0 = s0 + threadIdx.x; i0 < s1; i0 += kRBuildBlock * kPrefetch) {
-            unsigned long long v[kPrefetch];
+        for (uint32_t i0 = s0 + threadIdx.x;; i0 += kRBuildBlock * kBuildRows) {
 #pragma unroll
-            for (int u = 0; u < kPrefetch; ++u) {
-                const uint32_t i = i0 + u * kRBuildBlock;
-                v[u] = i < s1 ? staging[i] : kEmptySlot;
-            }
-#pragma unroll
-            for (int u = 0; u < kPrefetch; ++u) {
+            for (int u = 0; u < kBuildRows; ++u) {
                 const uint32_t i = i0 + u * kRBuildBlock;
                 if (i >= s1) continue;
                 const uint32_t hb = home_bucket((int32_t)(uint32_t)v[u], sj.t) - b0;
-                if (region_insert(tab, nb, hb, v[u], dup)) ++ins;
+                if (region_insert(tab, fill, nb, hb, v[u])) ++ins;
                 else ovf[atomicAdd(ovf_count, 1u)] = ((unsigned long long)j << 32) | i;  // the run leaves the region
             }
+            if (i0 + kRBuildBlock * kBuildRows >= s1) break;
+            load_region_rows(staging, i0 + kRBuildBlock * kBuildRows - threadIdx.x, s1, v);  // a large region
         }
+        __syncthreads();
+        const uint32_t gn = next_region(g + gridDim.x, regions, start, fresh);
+        if (gn < regions) load_region_rows(staging, start[gn], start[gn + 1], v);  // in flight from here on
+        bool dup = false;
+        for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) dup |= bucket_has_dup(tab, fill, nb, b);
         fence_proxy_async_smem();  // the inserts, before the bulk store reads them
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -302,6 +497,7 @@ __global__ void __launch_bounds__(kRBuildBlock) k_region_build(const RegionJob* 
             if (tot) atomicAdd(sj.t.meta + 2, tot);
             if (any_dup) atomicOr(sj.t.meta + 3, 1ull);
         }
+        g = gn;
     }
     if (threadIdx.x == 0) bulk_wait_all();  // every region store is complete before the CTA ends
 }
@@ -351,15 +547,19 @@ RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows) 
 cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0, uint32_t njobs,
                                  const BatchItem* items, uint32_t nitems, uint64_t n, uint64_t rows_per_item,
                                  uint32_t total_regions, uint32_t max_job_regions, const RegionScratch& sc,
-                                 bool fresh, cudaStream_t s, Context* ctx) {
+                                 bool fresh, bool partitioned, cudaStream_t s, Context* ctx) {
     if (total_regions == 0) return cudaSuccess;
     if (!items) nitems = (uint32_t)((n + rows_per_item - 1) / rows_per_item);
     const int sms = ctx->prop.multiProcessorCount;
     const size_t hsmem = 4ull * std::max(max_job_regions, 1u);
-    const size_t tsmem = 32ull * kRegionBuckets;
+    const bool sorted = partitioned && !items && njobs == 1;
+    const size_t wsmem = sizeof(WarpSort) * (kRBlock / 32);
+    const size_t tsmem = (32ull + 4ull) * kRegionBuckets;  // the region, then its fill counters
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_region_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
         (e = cudaFuncSetAttribute(k_region_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
+        (e = cudaFuncSetAttribute(k_region_scatter_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wsmem)) ||
         (e = cudaFuncSetAttribute(k_region_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)))
         return e;
     if ((e = cudaMemsetAsync(sc.hist, 0, 4ull * total_regions, s))) return e;
@@ -374,7 +574,15 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
     k_region_scan<<<1, kScanBlock, 0, s>>>(sc.hist, total_regions, sc.start, sc.cursor);
     ctx->launches++;
     if ((e = cudaGetLastError())) return e;
-    if (nitems) {
+    if (sorted && n) {
+        const uint64_t tiles = (n + kWarpTile - 1) / kWarpTile;
+        const uint64_t ctas = (tiles + kRBlock / 32 - 1) / (kRBlock / 32);
+        const int grid = (int)std::min<uint64_t>(
+            ctas, (uint64_t)occupancy_grid((const void*)k_region_scatter_sorted, kRBlock, wsmem, ctx));
+        k_region_scatter_sorted<<<grid, kRBlock, wsmem, s>>>(job0, n, sc.cursor, sc.staging, ctx->d_err);
+        ctx->launches++;
+        if ((e = cudaGetLastError())) return e;
+    } else if (nitems) {
         const int grid = (int)std::min<uint64_t>(
             nitems, (uint64_t)occupancy_grid((const void*)k_region_scatter, kRBlock, hsmem, ctx));
         k_region_scatter<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.cursor,

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 
@@ -73,6 +74,43 @@ static mgv_status check_device(Context* ctx, cudaStream_t s) {
 
 static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t ncols, uint64_t n, cudaStream_t s);
 
+namespace mgv {
+
+// Group rows in ascending group order: an LSD radix sort on the biased key,
+// three passes of 11 bits, a pass skipped when every key has the same digit
+// (small group ids use one or two passes).  A comparison sort of 4096 rows
+// took about 180 us on the host, longer than the query's own close.
+void sort_group_rows(std::vector<mgv_group_row>& v) {
+    const size_t n = v.size();
+    if (n < 64) {
+        std::sort(v.begin(), v.end(), [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+        return;
+    }
+    auto digit = [](const mgv_group_row& r, int pass) { return (((uint32_t)r.group ^ 0x80000000u) >> (11 * pass)) & 2047u; };
+    static thread_local std::vector<uint32_t> cnt;  // the three digit histograms, from one read
+    cnt.assign(3 * 2048, 0u);
+    for (size_t i = 0; i < n; ++i)
+        for (int pass = 0; pass < 3; ++pass) ++cnt[2048 * pass + digit(v[i], pass)];
+    std::unique_ptr<mgv_group_row[]> tmp(new mgv_group_row[n]);
+    mgv_group_row* src = v.data();
+    mgv_group_row* dst = tmp.get();
+    for (int pass = 0; pass < 3; ++pass) {
+        uint32_t* c = cnt.data() + 2048 * pass;
+        if (c[digit(src[0], pass)] == n) continue;  // every key has this digit: the order stands
+        uint32_t sum = 0;
+        for (int d = 0; d < 2048; ++d) {
+            const uint32_t x = c[d];
+            c[d] = sum;
+            sum += x;
+        }
+        for (size_t i = 0; i < n; ++i) dst[c[digit(src[i], pass)]++] = src[i];
+        std::swap(src, dst);
+    }
+    if (src != v.data()) std::copy(src, src + n, v.data());
+}
+
+}  // namespace mgv
+
 // A terminal group-by's close: its groups are packed on the device and come
 // back with the error word in one copy to pinned memory and one
 // synchronisation, then are ordered by group.
@@ -98,8 +136,7 @@ static mgv_status close_groupby(Op* o, cudaStream_t s) {
         MGV_CUDA_TRY(cudaMemcpy(o->gb_rows.data() + o->gb_land_rows, o->gb_dev_rows + o->gb_land_rows,
                                 sizeof(mgv_group_row) * (size_t)(n - o->gb_land_rows), cudaMemcpyDeviceToHost));
     }
-    std::sort(o->gb_rows.begin(), o->gb_rows.end(),
-              [](const mgv_group_row& x, const mgv_group_row& y) { return x.group < y.group; });
+    sort_group_rows(o->gb_rows);
     return MGV_OK;
 }
 
@@ -539,7 +576,9 @@ mgv_status mgv_op_create_partition(mgv_ctx* ctx, const mgv_partition_desc* d, mg
     o->pt = *d;
     o->parent = parent;
     mgv_status st = dev_alloc(o, (void**)&o->pt_dev, sizeof(unsigned long long) << d->radix_bits);
+    if (st == MGV_OK) st = dev_alloc(o, (void**)&o->pt_acc, sizeof(unsigned long long) * ((1ull << d->radix_bits) + 1));
     if (st != MGV_OK) {
+        for (void* p : o->allocs) cudaFree(p);
         delete o;
         return st;
     }
@@ -636,8 +675,8 @@ static mgv_status op_reset(Op* o, cudaStream_t s) {
             break;
         case OpKind::Partition:
             o->pt_fill = 0;
-            o->pt_runs.clear();
             o->pt_hist.assign((size_t)1 << o->pt.radix_bits, 0);
+            MGV_CUDA_TRY(cudaMemsetAsync(o->pt_acc, 0, sizeof(unsigned long long) * (o->pt_hist.size() + 1), s));
             break;
         default: break;
     }
@@ -736,12 +775,26 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
         return st;
     }
     if (o->kind == OpKind::Partition) {
-        // push the stored rows, partition by partition, into the parent chain
-        for (const auto& run : o->pt_runs) {
+        // the device's totals (and any overflow of max_rows), then the stored
+        // rows -- every consume's run partition-major -- go to the parent chain;
+        // a hash build on the same radix bits scatters them by sorted warp tiles
+        st = check_device(o->ctx, s);
+        if (st == MGV_OK) {
+            std::vector<unsigned long long> acc(o->pt_hist.size() + 1);
+            MGV_CUDA_TRY(cudaMemcpy(acc.data(), o->pt_acc, sizeof(unsigned long long) * acc.size(),
+                                    cudaMemcpyDeviceToHost));
+            o->pt_fill = acc[0];
+            for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = acc[1 + p];
+        }
+        if (st == MGV_OK && o->pt_fill) {
+            Op* hb = o->parent;
+            hb->hb_partitioned = hb->kind == OpKind::HashBuild && hb->hb.key_col == o->pt.key_col &&
+                                 hb->table.radix_mask == (1u << o->pt.radix_bits) - 1u &&
+                                 hb->table.radix_shift == o->pt.radix_shift;
             const int32_t* cols[MGV_MAX_COLS];
-            for (uint32_t c = 0; c < o->pt_ncols; ++c) cols[c] = o->pt_store + c * o->pt.max_rows + run.first;
-            st = consume_cols(o->parent, cols, o->pt_ncols, run.second, s);
-            if (st != MGV_OK) break;
+            for (uint32_t c = 0; c < o->pt_ncols; ++c) cols[c] = o->pt_store + c * o->pt.max_rows;
+            st = consume_cols(o->parent, cols, o->pt_ncols, o->pt_fill, s);
+            hb->hb_partitioned = false;
         }
     }
     mgv_status st2 = mgv_op_close(static_cast<mgv_op*>(o->parent), stream);  // after_close
@@ -854,7 +907,8 @@ static bool all_open(Op* o) {
 
 }  // extern "C"
 
-// Partition consume: histogram, prefix sums, scatter into the op's store.
+// Partition consume: histogram, cursors and scatter into the op's store, all
+// on the device (the totals are read back once, at close).
 static mgv_status consume_partition(Op* part, Op* sel, const int32_t* const* cols, uint32_t ncols, uint64_t n,
                                     cudaStream_t s) {
     Context* ctx = part->ctx;
@@ -870,26 +924,11 @@ static mgv_status consume_partition(Op* part, Op* sel, const int32_t* const* col
     MGV_CUDA_TRY(launch_partition_hist(cols, n, sel != nullptr, sel ? sel->sel.col : 0, sel ? sel->sel.bound : 0,
                                        part->pt.key_col, part->pt.radix_shift, part->pt.radix_bits, part->pt_dev, s,
                                        ctx));
-    std::vector<unsigned long long> hist(P);
-    MGV_CUDA_TRY(cudaMemcpyAsync(hist.data(), part->pt_dev, 8ull * P, cudaMemcpyDeviceToHost, s));
-    MGV_CUDA_TRY(cudaStreamSynchronize(s));
-    uint64_t rows = 0;
-    std::vector<unsigned long long> cursor(P);
-    for (uint32_t p = 0; p < P; ++p) {
-        cursor[p] = part->pt_fill + rows;
-        rows += hist[p];
-        part->pt_hist[p] += hist[p];
-    }
-    if (part->pt_fill + rows > part->pt.max_rows)
-        return fail(MGV_ENOMEM, "partition: more rows than max_rows");
-    MGV_CUDA_TRY(cudaMemcpyAsync(part->pt_dev, cursor.data(), 8ull * P, cudaMemcpyHostToDevice, s));
+    MGV_CUDA_TRY(launch_partition_cursors(part->pt_dev, part->pt.radix_bits, part->pt_acc, part->pt.max_rows, s, ctx));
     MGV_CUDA_TRY(launch_partition_scatter(cols, ncols, n, sel != nullptr, sel ? sel->sel.col : 0,
                                           sel ? sel->sel.bound : 0, part->pt.key_col, part->pt.radix_shift,
                                           part->pt.radix_bits, part->pt_dev, part->pt_store, part->pt.max_rows, s,
                                           ctx));
-    MGV_CUDA_TRY(cudaStreamSynchronize(s));  // the host cursors above must outlive the copy
-    if (rows) part->pt_runs.emplace_back(part->pt_fill, rows);
-    part->pt_fill += rows;
     return MGV_OK;
 }
 
@@ -1014,7 +1053,8 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
             const uint64_t rows_per_item =
                 std::max<uint64_t>({8ull * regions, 4096, n / (2ull * ctx->prop.multiProcessorCount) + 1});
             MGV_CUDA_TRY(launch_build_regions(nullptr, job, 1, nullptr, 0, n, rows_per_item, regions, regions,
-                                              carve_region_scratch(term->rb_scratch, regions, n), fresh, s, ctx));
+                                              carve_region_scratch(term->rb_scratch, regions, n), fresh,
+                                              term->hb_partitioned && !sel, s, ctx));
             return MGV_OK;
         }
         case OpKind::Partition: {

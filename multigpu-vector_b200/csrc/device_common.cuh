@@ -106,6 +106,49 @@ __device__ __forceinline__ void block_accumulate2(unsigned long long a, unsigned
     }
 }
 
+// In-place exclusive prefix sum of a[0..n) in shared memory over a CTA of
+// BLOCK threads; returns the total.  Every thread of the CTA calls it; a[] is
+// complete and the scratch free again when it returns.
+template <int BLOCK, typename T = uint32_t>
+__device__ __forceinline__ T block_exclusive_scan(T* a, uint32_t n) {
+    static_assert(BLOCK % kWarp == 0 && BLOCK / kWarp <= kWarp, "one warp scans the warp totals");
+    __shared__ T wsum[BLOCK / kWarp];
+    const uint32_t per = (n + BLOCK - 1) / BLOCK;
+    const uint32_t lo = threadIdx.x * per;
+    const uint32_t lane = lane_id(), warp = threadIdx.x / kWarp;
+    T local = 0;
+    for (uint32_t i = 0; i < per; ++i)
+        if (lo + i < n) local += a[lo + i];
+    T x = local;  // inclusive scan over the warp
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == kWarp - 1) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < BLOCK / kWarp ? wsum[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const T y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        if (lane < BLOCK / kWarp) wsum[lane] = w;
+    }
+    __syncthreads();
+    T base = (warp ? wsum[warp - 1] : T(0)) + x - local;
+    for (uint32_t i = 0; i < per; ++i)
+        if (lo + i < n) {
+            const T c = a[lo + i];
+            a[lo + i] = base;
+            base += c;
+        }
+    const T total = wsum[BLOCK / kWarp - 1];
+    __syncthreads();
+    return total;
+}
+
 }  // namespace mgv
 
 namespace mgv {

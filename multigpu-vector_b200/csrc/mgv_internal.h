@@ -167,11 +167,12 @@ struct Op {
     mgv_partition_desc pt{};
     int32_t* pt_store = nullptr;          // ncols x capacity, partition-major runs
     uint32_t pt_ncols = 0;
-    uint64_t pt_fill = 0;                 // rows stored
-    unsigned long long* pt_dev = nullptr; // [P] histogram / cursors
-    std::vector<uint64_t> pt_hist;        // rows per partition (all runs)
-    std::vector<std::pair<uint64_t, uint64_t>> pt_runs;  // (first row, rows)
+    uint64_t pt_fill = 0;                 // rows stored (read back at close)
+    unsigned long long* pt_dev = nullptr; // [P] histogram / cursors of a consume
+    unsigned long long* pt_acc = nullptr; // [1 + P] rows stored, rows per partition
+    std::vector<uint64_t> pt_hist;        // rows per partition (read back at close)
     bool hb_fresh = false;  // opened, nothing consumed yet: the table is not cleared yet
+    bool hb_partitioned = false;  // the rows being consumed are a partition op's run on the table's radix bits
     // shared-memory build scratch (hash_build), grown on demand
     void* rb_scratch = nullptr;
     size_t rb_bytes = 0;
@@ -286,16 +287,20 @@ struct RegionScratch {
     unsigned long long* staging;  // [rows] {key, payload}, region-major
     unsigned long long* ovf;  // [rows] job << 32 | staging row, left for the global insert
 };
+// Host: group rows in ascending group order (radix sort).
+void sort_group_rows(std::vector<mgv_group_row>& v);
 inline uint32_t table_regions(const TableView& t) { return (t.nbuckets + kRegionBuckets - 1) / kRegionBuckets; }
 size_t region_scratch_bytes(uint32_t regions, uint64_t rows);
 RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows);
 // Items: explicit (job, rows) items, or (items == nullptr) rows [0, n) of
 // job0 cut into items of rows_per_item.  fresh: the tables hold nothing yet
-// and are not cleared beforehand; every region is written.
+// and are not cleared beforehand; every region is written.  partitioned
+// (one job, no items): the rows arrive partitioned on the table's radix bits,
+// and are scattered by warps that sort their tiles by region.
 cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0, uint32_t njobs,
                                  const struct BatchItem* items, uint32_t nitems, uint64_t n, uint64_t rows_per_item,
                                  uint32_t total_regions, uint32_t max_job_regions, const RegionScratch& sc,
-                                 bool fresh, cudaStream_t s, Context* ctx);
+                                 bool fresh, bool partitioned, cudaStream_t s, Context* ctx);
 
 struct BatchOut {  // packed result region of a query
     GroupTableView gt;
@@ -314,6 +319,8 @@ cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const Bat
 cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,
                                   int32_t sel_bound, uint32_t key_col, uint32_t shift, uint32_t bits,
                                   unsigned long long* hist, cudaStream_t s, Context* ctx);
+cudaError_t launch_partition_cursors(unsigned long long* hc, uint32_t bits, unsigned long long* acc, uint64_t max_rows,
+                                    cudaStream_t s, Context* ctx);
 cudaError_t launch_partition_scatter(const int32_t* const* cols, uint32_t ncols, uint64_t n, bool has_sel,
                                      uint32_t sel_col, int32_t sel_bound, uint32_t key_col, uint32_t shift,
                                      uint32_t bits, unsigned long long* cursors, int32_t* out, uint64_t out_stride,

@@ -312,6 +312,38 @@ def test_shared_memory_build(ctx, torch_cuda, lf, build_filter):
         o.destroy()
 
 
+@pytest.mark.parametrize("lf", [0.5, 0.95])
+@pytest.mark.parametrize("seed", range(4))
+def test_shared_memory_build_one_duplicate_pair(ctx, torch_cuda, lf, seed):
+    """Unique keys except for one pair.  The region build claims slots by
+    per-bucket fill counters and finds duplicates in a pass afterwards, over
+    each bucket and the full buckets after it; at load factor 0.95 many runs
+    span several buckets, so the two copies often sit in different buckets.
+    A pair the pass missed would mark the table unique, and the probe would
+    stop at the first of the two matches."""
+    nb, npb = 1 << 18, 1 << 19
+    bk = po.gen_perm(nb, 0x5EED0700 + seed)
+    rng = np.random.default_rng(0x5EED0710 + seed)
+    i, j = rng.choice(nb, 2, replace=False)
+    bk[j] = bk[i]
+    bp = po.gen_uniform(nb, 0x5EED0720 + seed, 1, 0, 1 << 20)
+    pk = po.gen_uniform(npb, 0x5EED0730 + seed, 0, 0, nb)
+    pk[:64] = bk[i]
+    pp = po.gen_uniform(npb, 0x5EED0730 + seed, 1, 0, 1 << 20)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp, load_factor=lf)
+    assert info.has_duplicates == 1 and info.rows == nb
+    assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+
+
+def test_shared_memory_build_unique_full_table(ctx, torch_cuda):
+    """Unique keys at load factor 0.95: long runs of full buckets, no false
+    duplicate."""
+    bk, bp, pk, pp, hits = config2_inputs(1 << 18, 1 << 19, seed=0x5EED0740)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp, load_factor=0.95)
+    assert info.has_duplicates == 0 and info.rows == 1 << 18
+    assert cnt == hits and (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+
+
 def test_shared_memory_build_unique_keys(ctx, torch_cuda):
     """A region-built table of unique keys is reported duplicate-free (so the
     probe stops at the first match) and joins exactly."""

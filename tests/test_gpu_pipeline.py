@@ -99,6 +99,30 @@ def test_partition_histogram_and_rows(ctx, torch_cuda):
     pool.destroy()
 
 
+def test_partition_more_rows_than_max_rows_is_reported(ctx, torch_cuda):
+    """The partition's cursors are computed on the device, so a consume past
+    max_rows is reported by close (rows past the store are dropped, none is
+    written out of it); the operator then works again after reopening."""
+    torch = torch_cuda
+    n = 50000
+    k = po.gen_uniform(n, 0x5EED0903, 0, -(1 << 31), 1 << 32)
+    pool = mgv.Pool(ctx, 4, 1 << 15, 1)
+    sink = mgv.Op.sink(ctx, pool)
+    part = mgv.Op.partition(ctx, 0, 4, 0, n - 1, sink)
+    part.open()
+    part.consume_columns([dev(torch, k)], n)
+    with pytest.raises(mgv.MgvError) as e:
+        part.close()
+    assert e.value.status == mgv.ENOMEM
+    part.open()
+    part.consume_columns([dev(torch, k[:n - 1])], n - 1)
+    part.close()
+    assert sum(part.result()) == n - 1 and sink.result() == n - 1
+    for o in (part, sink):
+        o.destroy()
+    pool.destroy()
+
+
 def test_select_partition_aggregate(ctx, torch_cuda):
     n = 100000
     f = po.gen_uniform(n, 0x5EED0903, 0, 0, 100)
