@@ -413,7 +413,10 @@ typedef struct mgv_server_config {
     uint32_t max_inflight;   /* batches on the GPU at once (0 = 2, max 16)    */
     float load_factor;       /* resident join tables (0 = context default)    */
     uint32_t plain;          /* 1 = one request at a time, operator API       */
-    uint32_t reserved[2];
+    uint32_t batch_solo;     /* 0: a request that arrives to an idle server
+                              * runs alone through the operator chain (lower
+                              * latency); 1: it is batched like any other     */
+    uint32_t reserved;
 } mgv_server_config;
 
 typedef struct mgv_server_request {
@@ -430,6 +433,7 @@ typedef struct mgv_server_stats {
     double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result on the host */
     double mean_batch;
     uint64_t resident_table_bytes, peak_bytes;
+    uint64_t solo;           /* requests answered alone by the operator chain */
 } mgv_server_stats;
 
 typedef struct mgv_server mgv_server;

@@ -400,12 +400,8 @@ mgv_status mgv_batch_run_plain(mgv_batch* b, void* stream) {
         if (st != MGV_OK) return st;
     }
     b->last_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    for (uint32_t i = 0; i < nq; ++i) {
-        size_t need = 0;
-        mgv_op_result(b->plain[i].gb, nullptr, 0, &need);
-        b->plain[i].rows.resize(need / sizeof(mgv_group_row));
-        mgv_op_result(b->plain[i].gb, b->plain[i].rows.data(), need, nullptr);
-    }
+    // kept as closed (unordered); ordered when read, as the batch's own rows
+    for (uint32_t i = 0; i < nq; ++i) b->plain[i].rows = static_cast<Op*>(b->plain[i].gb)->gb_rows;
     return MGV_OK;
 }
 
@@ -416,6 +412,7 @@ mgv_status mgv_batch_result(mgv_batch* b, uint32_t q, int plain, mgv_group_row* 
     if (plain) {
         if (b->plain.empty()) return fail(MGV_ESTATE, "the plain pipeline has not run");
         v = b->plain[q].rows;
+        sort_rows(v);
     } else {
         if (!b->warmed) return fail(MGV_ESTATE, "the batch has not run");
         const uint32_t n = std::min<uint32_t>(b->h_counts[q], b->q[q].max_groups);

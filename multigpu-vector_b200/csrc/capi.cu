@@ -113,7 +113,7 @@ void sort_group_rows(std::vector<mgv_group_row>& v) {
 
 // A terminal group-by's close: its groups are packed on the device and come
 // back with the error word in one copy to pinned memory and one
-// synchronisation, then are ordered by group.
+// synchronisation.  They are ordered by group when first read.
 static mgv_status close_groupby(Op* o, cudaStream_t s) {
     Context* ctx = o->ctx;
     unsigned char* h = o->gb_land;
@@ -136,7 +136,7 @@ static mgv_status close_groupby(Op* o, cudaStream_t s) {
         MGV_CUDA_TRY(cudaMemcpy(o->gb_rows.data() + o->gb_land_rows, o->gb_dev_rows + o->gb_land_rows,
                                 sizeof(mgv_group_row) * (size_t)(n - o->gb_land_rows), cudaMemcpyDeviceToHost));
     }
-    sort_group_rows(o->gb_rows);
+    o->gb_sorted = false;  // ordered by group when first read (mgv_op_result)
     return MGV_OK;
 }
 
@@ -810,7 +810,14 @@ mgv_status mgv_op_result(mgv_op* o, void* out, size_t bytes, size_t* needed) {
         case OpKind::Aggregate: src = &o->agg_result; n = sizeof(o->agg_result); break;
         case OpKind::HashBuild: src = &o->hb_info; n = sizeof(o->hb_info); break;
         case OpKind::Sink: src = &o->sink_rows; n = sizeof(o->sink_rows); break;
-        case OpKind::Groupby: src = o->gb_rows.data(); n = o->gb_rows.size() * sizeof(mgv_group_row); break;
+        case OpKind::Groupby:
+            if (!o->gb_sorted) {
+                sort_group_rows(o->gb_rows);
+                o->gb_sorted = true;
+            }
+            src = o->gb_rows.data();
+            n = o->gb_rows.size() * sizeof(mgv_group_row);
+            break;
         case OpKind::Partition: src = o->pt_hist.data(); n = o->pt_hist.size() * sizeof(uint64_t); break;
         default: return fail(MGV_EINVAL, "operator has no result");
     }

@@ -159,6 +159,7 @@ struct Op {
     mgv_groupby_desc gb{};
     GroupTableView gtab{};
     std::vector<mgv_group_row> gb_rows;
+    bool gb_sorted = false;  // gb_rows ordered by group (done at the first result read)
     mgv_group_row* gb_dev_rows = nullptr;  // [cap + 1] packed by close()
     uint32_t* gb_dev_count = nullptr;
     unsigned char* gb_land = nullptr;      // pinned: {err[2], count, pad} then kGroupLandRows rows

@@ -109,7 +109,7 @@ struct mgv_server {
     std::thread th;
     // stats
     std::vector<double> latencies;
-    uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0;
+    uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0, solo = 0;
     // plain mode: group-by operators (device tables) reused per max_groups
     std::map<uint32_t, mgv_op*> plain_gb;
     std::vector<std::unique_ptr<Landing>> landings;  // pinned result buffers (lock held)
@@ -317,12 +317,7 @@ mgv_status run_plain(mgv_server* S, Request& q) {
     if (st == MGV_OK) st = mgv_op_open(sel, nullptr);
     if (st == MGV_OK) st = mgv_op_consume_columns(sel, cols, 4, r.probe_rows, nullptr);
     if (st == MGV_OK) st = mgv_op_close(sel, nullptr);
-    if (st == MGV_OK) {
-        size_t need = 0;
-        mgv_op_result(gb, nullptr, 0, &need);
-        q.rows.resize(need / sizeof(mgv_group_row));
-        mgv_op_result(gb, q.rows.data(), need, nullptr);
-    }
+    if (st == MGV_OK) q.rows = static_cast<Op*>(gb)->gb_rows;  // in no particular order, as the batched server's
     mgv_op_destroy(sel);
     mgv_op_destroy(probe);
     return st;
@@ -357,8 +352,28 @@ void scheduler(mgv_server* S) {
         Inflight* free_slot = nullptr;
         for (auto& sl : S->slots)
             if (!sl.busy) { free_slot = &sl; break; }
+        const size_t budget = S->cfg.memory_budget > S->table_bytes ? S->cfg.memory_budget - S->table_bytes : 0;
+        if (!any_busy && !S->cfg.batch_solo && S->pending.size() == 1 &&
+            S->used + S->pending.front()->bytes <= budget) {
+            // a lone request on an idle server: the single-query chain answers
+            // it without batch planning or event polling (admitted and charged
+            // like a batch of one)
+            auto q = S->pending.front();
+            S->pending.pop_front();
+            S->used += q->bytes;
+            S->peak = std::max(S->peak, S->used + S->table_bytes);
+            lk.unlock();
+            const mgv_status st = run_plain(S, *q);
+            lk.lock();
+            S->used -= q->bytes;
+            S->batches++;
+            S->batched_queries++;
+            S->solo++;
+            complete(S, q, st);
+            S->done_cv.notify_all();
+            continue;
+        }
         if (free_slot && !S->pending.empty()) {
-            const size_t budget = S->cfg.memory_budget > S->table_bytes ? S->cfg.memory_budget - S->table_bytes : 0;
             while (!S->pending.empty() && free_slot->reqs.size() < S->cfg.max_batch) {
                 auto& q = S->pending.front();
                 if (q->bytes > budget) {  // can never fit
@@ -509,6 +524,7 @@ mgv_status mgv_server_stats_get(mgv_server* S, mgv_server_stats* out) {
     out->batches = S->batches;
     out->rejected = S->rejected;
     out->mean_batch = S->batches ? (double)S->batched_queries / S->batches : 0.0;
+    out->solo = S->solo;
     out->resident_table_bytes = S->table_bytes;
     out->peak_bytes = S->peak;
     if (!S->latencies.empty()) {
@@ -529,7 +545,7 @@ mgv_status mgv_server_reset_stats(mgv_server* S) {
     if (!S) return fail(MGV_EINVAL, "server is NULL");
     std::lock_guard<std::mutex> lk(S->mu);
     S->latencies.clear();
-    S->submitted = S->completed = S->batches = S->rejected = S->batched_queries = 0;
+    S->submitted = S->completed = S->batches = S->rejected = S->batched_queries = S->solo = 0;
     S->peak = S->used + S->table_bytes;
     return MGV_OK;
 }

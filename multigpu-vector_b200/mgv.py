@@ -121,7 +121,7 @@ class BatchStats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget", c_uint64), ("max_batch", c_uint32), ("max_inflight", c_uint32),
-                ("load_factor", c_float), ("plain", c_uint32), ("reserved", c_uint32 * 2)]
+                ("load_factor", c_float), ("plain", c_uint32), ("batch_solo", c_uint32), ("reserved", c_uint32)]
 
 
 class ServerRequest(ctypes.Structure):
@@ -133,7 +133,8 @@ class ServerRequest(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("batches", c_uint64), ("rejected", c_uint64),
                 ("p50_ms", c_double), ("p99_ms", c_double), ("mean_ms", c_double), ("max_ms", c_double),
-                ("mean_batch", c_double), ("resident_table_bytes", c_uint64), ("peak_bytes", c_uint64)]
+                ("mean_batch", c_double), ("resident_table_bytes", c_uint64), ("peak_bytes", c_uint64),
+                ("solo", c_uint64)]
 
 
 class SinkDesc(ctypes.Structure):
@@ -538,9 +539,9 @@ class Server:
     """mgv_server: continuous batching over resident build tables."""
 
     def __init__(self, ctx: Context, memory_budget: int, max_batch: int = 0, max_inflight: int = 0,
-                 load_factor: float = 0.0, plain: bool = False):
+                 load_factor: float = 0.0, plain: bool = False, batch_solo: bool = False):
         h = c_void_p()
-        cfg = ServerConfig(memory_budget, max_batch, max_inflight, load_factor, int(plain))
+        cfg = ServerConfig(memory_budget, max_batch, max_inflight, load_factor, int(plain), int(batch_solo))
         _call("mgv_server_create", ctx.h, byref(cfg), byref(h))
         self.h, self.ctx = h, ctx
 

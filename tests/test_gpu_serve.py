@@ -46,12 +46,16 @@ def submit(server, r):
     return server.submit(tid, cols[1], cols[2], cols[3], cols[4], rows, bound, 4096)
 
 
-def test_alone_equals_in_the_mix(ctx, torch_cuda):
-    s = mgv.Server(ctx, 8 << 30, max_batch=64, max_inflight=2)
+@pytest.mark.parametrize("batch_solo", [False, True])
+def test_alone_equals_in_the_mix(ctx, torch_cuda, batch_solo):
+    """A request alone on an idle server runs through the single-query
+    operator chain (batch_solo False) or as a batch of one (True); either way
+    its groups equal those it gets batched with 59 others."""
+    s = mgv.Server(ctx, 8 << 30, max_batch=64, max_inflight=2, batch_solo=batch_solo)
     tabs = setup_tables(ctx, torch_cuda, s)
     reqs = requests(tabs, 60, 5)
     alone = []
-    for r in reqs:  # one at a time: each runs as a batch of one
+    for r in reqs:  # one at a time
         st, rows, _ = s.wait(submit(s, r))
         assert st == mgv.OK
         alone.append(rows)
@@ -66,6 +70,7 @@ def test_alone_equals_in_the_mix(ctx, torch_cuda):
         assert alone[i] == oracle(nbs[tid], cols, rows_n, bound), i
     st = s.stats()
     assert st.completed == 120 and st.batches < 120  # the mix was batched
+    assert (st.solo == 0) if batch_solo else (st.solo >= 60)
     s.destroy()
 
 
