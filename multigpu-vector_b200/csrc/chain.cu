@@ -4,10 +4,11 @@
 //
 // one kernel per consume call.  Warp-ballot select as in
 // unstable_select::consume_warp (src/operators/select3.cu:19-85): each warp
-// takes 128-row windows, evaluates the predicate and compacts the qualifying
-// rows with __ballot_sync / __popc into a per-warp shared-memory ring of 256
-// rows, carrying only the columns the rest of the chain reads (the others
-// are never loaded).  Full 128-row vectors then go through the probe and the
+// takes 512-row windows (16 filter loads per lane in flight), evaluates the
+// predicate and compacts the offsets of the qualifying rows with
+// __ballot_sync / __popc into a per-warp shared-memory ring of 1024 entries.
+// Every 128 offsets form a vector whose carried columns -- only those the
+// rest of the chain reads -- are gathered and handed to the probe and the
 // terminal (the reference's parent->consume_warp(x, 128)).
 //
 // The probe emits one output row per matching build row (all duplicates
@@ -15,11 +16,10 @@
 // is visible to the terminal as column `ncols`.
 //
 // Group-by (no reference counterpart): each CTA aggregates into a
-// shared-memory hash table; rows of equal group within a warp are first
-// combined with __match_any_sync + __reduce_add_sync, so a hot (Zipf) group
-// costs one shared atomic per warp instead of one per row.  Groups that do
-// not find a shared slot within a few probes go to the global table; at the
-// end of the CTA the shared table is merged into the global one.
+// shared-memory hash table with native 32-bit shared atomics (count, and the
+// int64 sum as two biased words).  Groups that do not find a shared slot
+// within a few probes, or arrive once the table is 5/8 full, go to the global
+// table; at the end of the CTA the shared table is merged into the global one.
 #include <cuda_runtime.h>
 
 #include "device_common.cuh"
