@@ -114,6 +114,10 @@ void sort_group_rows(std::vector<mgv_group_row>& v) {
 // A terminal group-by's close: its groups are packed on the device and come
 // back with the error word in one copy to pinned memory and one
 // synchronisation.  They are ordered by group when first read.
+// Group rows read back together with the count at a group-by's close; a
+// larger result costs one more copy (most results are smaller).
+constexpr uint32_t kGroupRowsFirstCopy = 4096;
+
 static mgv_status close_groupby(Op* o, cudaStream_t s) {
     Context* ctx = o->ctx;
     unsigned char* h = o->gb_land;
@@ -121,7 +125,9 @@ static mgv_status close_groupby(Op* o, cudaStream_t s) {
     MGV_CUDA_TRY(launch_group_pack(o->gtab, o->gb_dev_rows, o->gb_dev_count, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(h, ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaMemcpyAsync(h + 8, o->gb_dev_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    MGV_CUDA_TRY(cudaMemcpyAsync(h + 16, o->gb_dev_rows, sizeof(mgv_group_row) * (size_t)o->gb_land_rows,
+    // the first rows come with the count; a larger result follows after it
+    const uint32_t first = std::min<uint32_t>(o->gb_land_rows, kGroupRowsFirstCopy);
+    MGV_CUDA_TRY(cudaMemcpyAsync(h + 16, o->gb_dev_rows, sizeof(mgv_group_row) * (size_t)first,
                                  cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaStreamSynchronize(s));
     const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
@@ -130,11 +136,19 @@ static mgv_status close_groupby(Op* o, cudaStream_t s) {
     uint32_t n = 0;
     std::memcpy(&n, h + 8, sizeof(n));
     const mgv_group_row* rows = reinterpret_cast<const mgv_group_row*>(h + 16);
-    o->gb_rows.assign(rows, rows + std::min(n, o->gb_land_rows));
-    if (n > o->gb_land_rows) {  // more groups than the landing zone holds
+    o->gb_rows.assign(rows, rows + std::min(n, first));
+    if (n > first) {  // the rest, through the landing zone while it holds them
         o->gb_rows.resize(n);
-        MGV_CUDA_TRY(cudaMemcpy(o->gb_rows.data() + o->gb_land_rows, o->gb_dev_rows + o->gb_land_rows,
-                                sizeof(mgv_group_row) * (size_t)(n - o->gb_land_rows), cudaMemcpyDeviceToHost));
+        const uint32_t land_more = std::min(n, o->gb_land_rows) - first;
+        if (land_more) {
+            MGV_CUDA_TRY(cudaMemcpyAsync(h + 16, o->gb_dev_rows + first, sizeof(mgv_group_row) * (size_t)land_more,
+                                         cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            std::memcpy(o->gb_rows.data() + first, h + 16, sizeof(mgv_group_row) * (size_t)land_more);
+        }
+        if (n > o->gb_land_rows)
+            MGV_CUDA_TRY(cudaMemcpy(o->gb_rows.data() + o->gb_land_rows, o->gb_dev_rows + o->gb_land_rows,
+                                    sizeof(mgv_group_row) * (size_t)(n - o->gb_land_rows), cudaMemcpyDeviceToHost));
     }
     o->gb_sorted = false;  // ordered by group when first read (mgv_op_result)
     return MGV_OK;

@@ -295,20 +295,36 @@ void finish(mgv_server* S, Inflight& sl) {
 }
 
 // Plain mode: one request through the operator API (lock not held).
+// The group-by operator of the single-query chain for max_groups.  One per
+// power-of-two class: its table (2 x max_groups, rounded up to a power of two)
+// is the same for every max_groups of the class, so nothing is created per
+// request once the classes up to 2^16 exist (made with the server).
+uint32_t groupby_class(uint32_t max_groups) {
+    uint32_t c = 16;
+    while (c < max_groups) c <<= 1;
+    return c;
+}
+
+mgv_status plain_groupby(mgv_server* S, uint32_t max_groups, mgv_op** out) {
+    const uint32_t c = groupby_class(max_groups);
+    auto it = S->plain_gb.find(c);
+    if (it != S->plain_gb.end()) {
+        *out = it->second;
+        return MGV_OK;
+    }
+    mgv_groupby_desc gd{2, 3, c, 0};
+    mgv_status st = mgv_op_create_groupby(S->ctx, &gd, out);
+    if (st == MGV_OK) S->plain_gb[c] = *out;
+    return st;
+}
+
 mgv_status run_plain(mgv_server* S, Request& q) {
     const mgv_server_request& r = q.r;
     mgv_ctx* ctx = S->ctx;
     mgv_op *gb = nullptr, *probe = nullptr, *sel = nullptr;
     mgv_status st = MGV_OK;
-    auto it = S->plain_gb.find(r.max_groups);
-    if (it != S->plain_gb.end()) {
-        gb = it->second;
-    } else {
-        mgv_groupby_desc gd{2, 3, r.max_groups, 0};
-        st = mgv_op_create_groupby(ctx, &gd, &gb);
-        if (st != MGV_OK) return st;
-        S->plain_gb[r.max_groups] = gb;
-    }
+    st = plain_groupby(S, r.max_groups, &gb);
+    if (st != MGV_OK) return st;
     mgv_hash_probe_desc pd{0, 0, q.table};
     if (st == MGV_OK) st = mgv_op_create_hash_probe(ctx, &pd, gb, &probe);
     mgv_select_desc sd{1, r.filter_bound};
@@ -434,6 +450,15 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
     if (S->cfg.max_inflight == 0) S->cfg.max_inflight = 2;
     if (S->cfg.max_inflight > 16) S->cfg.max_inflight = 16;
     if (S->cfg.load_factor == 0.0f) S->cfg.load_factor = ctx->tuning.default_load_factor;
+    for (uint32_t c = 16; c <= (1u << 16); c <<= 1) {  // the single-query chain's group-by classes
+        mgv_op* gb = nullptr;
+        const mgv_status st = plain_groupby(S, c, &gb);
+        if (st != MGV_OK) {
+            for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
+            delete S;
+            return st;
+        }
+    }
     S->slots.resize(S->cfg.max_inflight);
     for (auto& sl : S->slots) {
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
