@@ -191,6 +191,8 @@ def main():
                     help="skip the batched and served summaries added to the join line (N = 1)")
     ap.add_argument("--load-factor", type=float, default=0.4,
                     help="join table load factor; 0.4 (an 80 MiB table for 2^22 keys) measured fastest")
+    ap.add_argument("--pipeline-load-factor", type=float, default=0.4,
+                    help="pipeline: load factor of the 2^24-key radix-partitioned table (0.4 measured fastest)")
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
     ap.add_argument("--no-e2e", action="store_true")

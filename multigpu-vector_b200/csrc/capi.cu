@@ -521,6 +521,8 @@ mgv_status mgv_op_create_hash_build(mgv_ctx* ctx, const mgv_hash_build_desc* d, 
     mgv_status st = dev_alloc(o, (void**)&t.slots, o->table_bytes);
     if (st == MGV_OK) st = dev_alloc(o, (void**)&t.meta, 4 * sizeof(unsigned long long));
     if (st == MGV_OK) st = dev_alloc(o, (void**)&t.side_pay, sizeof(int32_t) * t.side_cap);
+    if (st == MGV_OK && cudaMallocHost(&o->h_res, 5 * sizeof(unsigned long long)) != cudaSuccess)
+        st = fail(MGV_ENOMEM, "pinned host allocation");
     if (st != MGV_OK) {
         for (void* p : o->allocs) cudaFree(p);
         delete o;
@@ -591,6 +593,9 @@ mgv_status mgv_op_create_partition(mgv_ctx* ctx, const mgv_partition_desc* d, mg
     o->parent = parent;
     mgv_status st = dev_alloc(o, (void**)&o->pt_dev, sizeof(unsigned long long) << d->radix_bits);
     if (st == MGV_OK) st = dev_alloc(o, (void**)&o->pt_acc, sizeof(unsigned long long) * ((1ull << d->radix_bits) + 1));
+    if (st == MGV_OK &&
+        cudaMallocHost(&o->h_res, sizeof(unsigned long long) * ((1ull << d->radix_bits) + 2)) != cudaSuccess)
+        st = fail(MGV_ENOMEM, "pinned host allocation");
     if (st != MGV_OK) {
         for (void* p : o->allocs) cudaFree(p);
         delete o;
@@ -712,6 +717,17 @@ mgv_status mgv_op_open(mgv_op* o, void* stream) {
     return MGV_OK;
 }
 
+// A closed build's counters (meta[0..3] of the table) into its info.
+static void hash_build_info(Op* o, const unsigned long long* m) {
+    mgv_hash_build_info& i = o->hb_info;
+    i.rows = m[2] + m[0];
+    i.nbuckets = o->table.nbuckets;
+    i.table_bytes = o->table_bytes;
+    i.reserved_key_rows = m[0];
+    i.has_duplicates = (m[3] != 0 || m[0] > 1) ? 1u : 0u;
+    o->unique = m[3] == 0;
+}
+
 // Reads back a terminal operator's result after its stream completed.
 static mgv_status op_finish(Op* o, cudaStream_t s) {
     switch (o->kind) {
@@ -723,19 +739,7 @@ static mgv_status op_finish(Op* o, cudaStream_t s) {
             o->agg_result.sum = (int64_t)h[1];
             break;
         }
-        case OpKind::HashBuild: {
-            unsigned long long m[4];
-            MGV_CUDA_TRY(cudaMemcpyAsync(m, o->table.meta, sizeof(m), cudaMemcpyDeviceToHost, s));
-            MGV_CUDA_TRY(cudaStreamSynchronize(s));
-            mgv_hash_build_info& i = o->hb_info;
-            i.rows = m[2] + m[0];
-            i.nbuckets = o->table.nbuckets;
-            i.table_bytes = o->table_bytes;
-            i.reserved_key_rows = m[0];
-            i.has_duplicates = (m[3] != 0 || m[0] > 1) ? 1u : 0u;
-            o->unique = m[3] == 0;
-            break;
-        }
+
         case OpKind::Groupby: break;  // read back by close_groupby()
         case OpKind::Sink: {
             unsigned long long rows = 0;
@@ -783,6 +787,17 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
             return report_device_error(o->ctx, w, s);
         }
         if (o->kind == OpKind::Groupby) return close_groupby(o, s);
+        if (o->kind == OpKind::HashBuild) {  // the error word and the table's counters: one copy, one wait
+            unsigned long long* h = o->h_res;
+            MGV_CUDA_TRY(cudaMemcpyAsync(h, o->ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(h + 1, o->table.meta, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                         s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
+            st = report_device_error(o->ctx, w, s);
+            if (st == MGV_OK) hash_build_info(o, h + 1);
+            return st;
+        }
         st = check_device(o->ctx, s);
         mgv_status st2 = op_finish(o, s);
         if (st == MGV_OK) st = st2;
@@ -792,13 +807,16 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
         // the device's totals (and any overflow of max_rows), then the stored
         // rows -- every consume's run partition-major -- go to the parent chain;
         // a hash build on the same radix bits scatters them by sorted warp tiles
-        st = check_device(o->ctx, s);
+        unsigned long long* h = o->h_res;  // [error word, rows stored, rows per partition]: one copy, one wait
+        MGV_CUDA_TRY(cudaMemcpyAsync(h, o->ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        MGV_CUDA_TRY(cudaMemcpyAsync(h + 1, o->pt_acc, sizeof(unsigned long long) * (o->pt_hist.size() + 1),
+                                     cudaMemcpyDeviceToHost, s));
+        MGV_CUDA_TRY(cudaStreamSynchronize(s));
+        const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
+        st = report_device_error(o->ctx, w, s);
         if (st == MGV_OK) {
-            std::vector<unsigned long long> acc(o->pt_hist.size() + 1);
-            MGV_CUDA_TRY(cudaMemcpy(acc.data(), o->pt_acc, sizeof(unsigned long long) * acc.size(),
-                                    cudaMemcpyDeviceToHost));
-            o->pt_fill = acc[0];
-            for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = acc[1 + p];
+            o->pt_fill = h[1];
+            for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = h[2 + p];
         }
         if (st == MGV_OK && o->pt_fill) {
             Op* hb = o->parent;

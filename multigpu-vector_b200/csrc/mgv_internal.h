@@ -134,7 +134,7 @@ struct Op {
     // aggregate
     mgv_aggregate_desc agg{};
     unsigned long long* d_acc = nullptr;    // [count, sum]
-    unsigned long long* h_res = nullptr;    // pinned: [error word, count, sum]
+    unsigned long long* h_res = nullptr;    // pinned: the error word and the results read back at close
     mgv_agg_result agg_result{};
     // hash build
     mgv_hash_build_desc hb{};

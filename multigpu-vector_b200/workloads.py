@@ -108,7 +108,7 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
     ctx.gen_zipf(cols[2], npb, seed, 3, 4096, stream=stream)
     ctx.gen_uniform(cols[3], npb, seed, 4, 0, 1 << 16, stream=stream)
     qualifying = int((cols[1] <= 99).sum().item())
-    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8)
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8, args.pipeline_load_factor)
     bt, pt = [], []
     h0 = time.time()
     for i in range(args.warmup + args.steps):
@@ -149,7 +149,8 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
                      f"first 2^22 probe rows ({t_probe:.2f} s), scaled to 2^27 rows"}
     _line(args, "select->join->group-by probe rows/s", npb / (b + p_), "rows/s", 1000 * (b + p_),
           "select (filter <= 99 of U[0,1000)) -> join (2^27 probe rows, key over 2^24 build keys) -> group-by "
-          "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key bits",
+          "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key bits, "
+          f"table load factor {args.pipeline_load_factor}",
           {"roofline": {"bound": "hbm", "achieved": alg / (b + p_) / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": alg / (b + p_) / 1e9 / peak, "peak_kind": kind,
                         "algorithmic_bytes_per_step": alg},
