@@ -337,12 +337,19 @@ __device__ __forceinline__ int32_t pick_slot(const int32_t (&v)[NS][4], int32_t 
 // columns are gathered into registers (4 rows per lane, all loads
 // independent), its keys probed, and its rows handed to the terminal.  Only
 // qualifying rows' columns are ever loaded.
-template <bool SEL, bool PROBE, int TERM>
+template <bool SEL, bool PROBE, int TERM, bool FIXED = false>
 __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, uint64_t row_lo, uint64_t row_hi,
                                               uint64_t win_first, uint64_t win_stride, uint32_t* ids,
                                               const SmemGroups& sg, unsigned long long& acnt,
                                               unsigned long long& asum, uint32_t* err) {
     constexpr int NS = TERM == kTermSink ? MGV_MAX_COLS : kMaxTermSlots;
+    // A batch query's carried slots are fixed (FIXED): key, group, value from
+    // input columns 0, 2, 3, so every slot pick below resolves at compile time.
+    const uint32_t nslots = FIXED ? 3u : a.nslots;
+    const int32_t probe_slot = FIXED ? 0 : a.probe_slot;
+    const int32_t ref0 = FIXED ? 1 : a.ref[0];
+    const int32_t ref1 = FIXED ? 2 : a.ref[1];
+    auto slot_col = [&](int c) -> const int32_t* { return a.cols[FIXED ? (c == 0 ? 0 : c + 1) : a.slot_src[c]]; };
     const uint32_t lane = lane_id();
     const uint32_t len = (uint32_t)(row_hi - row_lo);
 
@@ -360,8 +367,8 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
         int32_t v[NS][4];
 #pragma unroll
         for (int c = 0; c < NS; ++c) {
-            const bool carried = (uint32_t)c < a.nslots;
-            const int32_t* col = carried ? a.cols[a.slot_src[c]] + row_lo : nullptr;
+            const bool carried = (uint32_t)c < nslots;
+            const int32_t* col = carried ? slot_col(c) + row_lo : nullptr;
 #pragma unroll
             for (int j = 0; j < 4; ++j) v[c][j] = (carried && in[j]) ? __ldg(col + rid[j]) : 0;
         }
@@ -374,15 +381,15 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
             if (TERM == kTermAgg) {
                 if (active) {
                     long long t = 0;
-                    if (a.ref[0] >= 0) t += val(a.ref[0], j, bp);
-                    if (a.ref[1] >= 0) t += val(a.ref[1], j, bp);
+                    if (ref0 >= 0) t += val(ref0, j, bp);
+                    if (ref1 >= 0) t += val(ref1, j, bp);
                     acnt += 1;
                     asum += (unsigned long long)t;
                 }
             } else if (TERM == kTermGroupby) {
                 if (active) {
-                    const int32_t g = val(a.ref[0], j, bp);
-                    const int32_t x = a.ref[1] >= 0 ? val(a.ref[1], j, bp) : 0;
+                    const int32_t g = val(ref0, j, bp);
+                    const int32_t x = ref1 >= 0 ? val(ref1, j, bp) : 0;
                     group_add_row(sg, a.gt, g, x, err);
                 }
             } else {
@@ -407,7 +414,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
             bool reserved_any = false;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                key[j] = pick_slot<NS>(v, a.probe_slot, j);
+                key[j] = pick_slot<NS>(v, probe_slot, j);
                 live[j] = in[j] && key[j] != kEmptyKey;
                 reserved_any |= in[j] && key[j] == kEmptyKey;
                 b[j] = home_bucket(key[j], a.table);
@@ -458,8 +465,8 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                     int32_t gg[4], gx[4];
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        gg[j] = val(a.ref[0], j, gbp[j]);
-                        gx[j] = a.ref[1] >= 0 ? val(a.ref[1], j, gbp[j]) : 0;
+                        gg[j] = val(ref0, j, gbp[j]);
+                        gx[j] = ref1 >= 0 ? val(ref1, j, gbp[j]) : 0;
                     }
                     group_add_rows4(sg, a.gt, gg, gx, gf, err);
                 }
@@ -582,7 +589,7 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* 
         }
         const ChainDev& a = sq;
         const bool unique = a.table.meta[3] == 0;
-        chain_windows<true, true, kTermGroupby>(a, unique, item.lo, item.hi, warp, kChainWarps,
+        chain_windows<true, true, kTermGroupby, true>(a, unique, item.lo, item.hi, warp, kChainWarps,
                                                 rings + (size_t)warp * kIdRing, sg, acnt, asum, err);
     }
     if (sg.cap) {
