@@ -125,6 +125,8 @@ void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
     S->completed++;
 }
 
+constexpr uint64_t kMinLandingRows = 1u << 18;  // 6 MiB of group rows
+
 // A free landing zone of at least `rows` rows and `ncounts` counts (scheduler
 // thread, lock not held; the list is read and changed under the lock, a new
 // zone is pinned outside it).
@@ -141,8 +143,10 @@ mgv_status acquire_landing(mgv_server* S, uint64_t rows, uint32_t ncounts, Landi
             return MGV_OK;
         }
     }
+    // pinning is slow (milliseconds for tens of MB): zones get headroom, so a
+    // later, larger batch finds one to reuse instead of pinning another
     auto L = std::make_unique<Landing>();
-    L->cap = rows + rows / 4;
+    L->cap = std::max<uint64_t>(rows + rows / 2, kMinLandingRows);
     L->ncounts = std::max<uint32_t>(ncounts, S->cfg.max_batch);
     void* p = nullptr;
     MGV_CUDA_TRY(cudaMallocHost(&p, sizeof(mgv_group_row) * L->cap + 4ull * L->ncounts));
@@ -458,6 +462,23 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
             delete S;
             return st;
         }
+    }
+    // landing zones pinned up front, so serving rarely pins (slow) while
+    // batches are in flight and waiters still hold earlier zones
+    for (uint32_t i = 0; i < 4 * S->cfg.max_inflight; ++i) {
+        auto L = std::make_unique<Landing>();
+        L->cap = kMinLandingRows;
+        L->ncounts = S->cfg.max_batch;
+        void* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(mgv_group_row) * L->cap + 4ull * L->ncounts) != cudaSuccess) {
+            for (auto& Z : S->landings) cudaFreeHost(Z->rows);
+            for (auto& kv : S->plain_gb) mgv_op_destroy(kv.second);
+            delete S;
+            return fail(MGV_ENOMEM, "pinned host allocation");
+        }
+        L->rows = static_cast<mgv_group_row*>(p);
+        L->counts = reinterpret_cast<uint32_t*>(L->rows + L->cap);
+        S->landings.push_back(std::move(L));
     }
     S->slots.resize(S->cfg.max_inflight);
     for (auto& sl : S->slots) {

@@ -370,29 +370,34 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
         srv.reset_stats()
         at, reqs = trace(rate, seed)
         # Results are drained by a second thread while requests arrive (the
-        # ctypes wait releases the GIL); each is kept as a digest of its rows.
-        tq: "queue.Queue[int | None]" = queue.Queue()
-        digests, errs = [], []
+        # ctypes wait releases the GIL).  It only waits: request i's rows land
+        # in its own slice of one preallocated array (its max_groups rows), so
+        # the drain keeps up with the server, and the digests are computed
+        # after the timed region.
+        caps = [tables[t][1] for t, _, _ in reqs]
+        offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+        res = np.empty((int(offs[-1]), 3), dtype=np.uint64)  # mgv_group_row = 3 x 64 bits
+        got = [0] * len(reqs)
+        tq: "queue.Queue[tuple[int, int] | None]" = queue.Queue()
+        errs = []
 
         def drain():
-            buf = (mgv.GroupRow * (1 << 16))()
             n, lat = ctypes.c_uint64(), ctypes.c_double()
+            base = res.ctypes.data
             while True:
-                tk = tq.get()
-                if tk is None:
+                item = tq.get()
+                if item is None:
                     return
-                st = mgv.load().mgv_server_wait(srv.h, tk, 600000, buf, 1 << 16, ctypes.byref(n), ctypes.byref(lat))
+                i, tk = item
+                st = mgv.load().mgv_server_wait(srv.h, tk, 600000, ctypes.c_void_p(base + 24 * int(offs[i])), caps[i],
+                                                ctypes.byref(n), ctypes.byref(lat))
                 if st != mgv.OK:
                     errs.append(st)
-                # order-independent digest of the rows (the server returns groups unordered)
-                rows = np.frombuffer(buf, dtype=np.uint64, count=3 * n.value).reshape(-1, 3)
-                mix = rows[:, 0] * np.uint64(0x9E3779B97F4A7C15) ^ rows[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F) \
-                    ^ rows[:, 2] * np.uint64(0x165667B19E3779F9)
-                digests.append((n.value, int(mix.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(mix))
-                                if n.value else 0))
+                got[i] = min(n.value, caps[i])
 
         th = threading.Thread(target=drain)
         th.start()
+        k_sub = [0]
         t0 = time.perf_counter()
         for a, (t, rows, bound) in zip(at, reqs):
             wait = a - (time.perf_counter() - t0)
@@ -401,12 +406,20 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
             while time.perf_counter() - t0 < a:
                 pass
             nb, g, bk, cols = tables[t]
-            tq.put(srv.submit(tids[t], *cols, rows, bound, g))
+            tq.put((k_sub[0], srv.submit(tids[t], *cols, rows, bound, g)))
+            k_sub[0] += 1
         t_sub = time.perf_counter() - t0
         tq.put(None)
         th.join()
         wall = time.perf_counter() - t0
         assert not errs, errs
+        # order-independent digest of each request's rows (the server returns groups unordered)
+        digests = []
+        for i in range(len(reqs)):
+            rows = res[offs[i]:offs[i] + got[i]]
+            mix = rows[:, 0] * np.uint64(0x9E3779B97F4A7C15) ^ rows[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F) \
+                ^ rows[:, 2] * np.uint64(0x165667B19E3779F9)
+            digests.append((got[i], int(mix.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(mix)) if got[i] else 0))
         stats = srv.stats()
         srv.destroy()
         return {"offered_qps": rate or None, "arrived_qps": len(reqs) / t_sub, "requests": len(reqs),
