@@ -59,6 +59,8 @@ cudaError_t launch_fill_u64(unsigned long long* p, uint64_t n, unsigned long lon
 // needs no compaction, so each thread folds 8 rows per 256-bit load.
 // ---------------------------------------------------------------------------
 
+constexpr int kSelVecs = 4;  // k_select_agg: 8-row vectors per thread per step
+
 template <bool SEL, bool HASA, bool HASB, bool VEC>
 __global__ void __launch_bounds__(kBlock) k_select_agg(const int32_t* __restrict__ f, int32_t bound,
                                                        const int32_t* __restrict__ a,
@@ -68,20 +70,30 @@ __global__ void __launch_bounds__(kBlock) k_select_agg(const int32_t* __restrict
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     uint64_t done = 0;
     if (VEC) {
+        // kSelVecs 8-row vectors per thread per step, every load issued before any is used
         const uint64_t nvec = n / 8;
-        for (uint64_t v = (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < nvec; v += stride) {
-            int32_t fv[8], av[8], bv[8];
-            if (SEL) ld_stream8(f + 8 * v, fv);
-            if (HASA) ld_stream8(a + 8 * v, av);
-            if (HASB) ld_stream8(b + 8 * v, bv);
+        for (uint64_t v0 = (uint64_t)blockIdx.x * kBlock + threadIdx.x; v0 < nvec; v0 += stride * kSelVecs) {
+            int32_t fv[kSelVecs][8], av[kSelVecs][8], bv[kSelVecs][8];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const bool p = !SEL || fv[r] <= bound;
-                long long t = 0;
-                if (HASA) t += av[r];
-                if (HASB) t += bv[r];
-                cnt += p;
-                sum += p ? (unsigned long long)t : 0ull;
+            for (int u = 0; u < kSelVecs; ++u) {
+                const uint64_t v = v0 + u * stride;
+                if (v >= nvec) continue;
+                if (SEL) ld_stream8(f + 8 * v, fv[u]);
+                if (HASA) ld_stream8(a + 8 * v, av[u]);
+                if (HASB) ld_stream8(b + 8 * v, bv[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < kSelVecs; ++u) {
+                if (v0 + u * stride >= nvec) continue;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const bool p = !SEL || fv[u][r] <= bound;
+                    long long t = 0;
+                    if (HASA) t += av[u][r];
+                    if (HASB) t += bv[u][r];
+                    cnt += p;
+                    sum += p ? (unsigned long long)t : 0ull;
+                }
             }
         }
         done = nvec * 8;
@@ -103,7 +115,9 @@ static cudaError_t select_agg_v(const int32_t* f, int32_t bound, const int32_t* 
     const bool vec = aligned32(f) && aligned32(a) && aligned32(b);
     const void* k = vec ? (const void*)k_select_agg<SEL, HASA, HASB, true>
                         : (const void*)k_select_agg<SEL, HASA, HASB, false>;
-    int grid = occupancy_grid(k, kBlock, 0, ctx);
+    // two CTAs per SM: enough loads in flight to fill HBM, and few CTAs adding
+    // into the one accumulator (same-address atomics serialise in L2)
+    int grid = std::min(occupancy_grid(k, kBlock, 0, ctx), 2 * ctx->prop.multiProcessorCount);
     uint64_t need = (n / 8 + kBlock - 1) / kBlock + 1;
     if ((uint64_t)grid > need) grid = (int)need;
     if (vec)
