@@ -47,6 +47,28 @@ def test_select_join_groupby(ctx, torch_cuda, radix_bits, nb, npb):
     assert info.rows == nb
 
 
+@pytest.mark.parametrize("radix_bits", [1, 2])
+def test_partitioned_build_wide_regions(ctx, torch_cuda, radix_bits):
+    """Few partitions of a large table: each partition spans over a hundred
+    shared-memory regions, so the warp tiles of the partition op's run span
+    more regions than a warp sorts and take the per-row cursor path."""
+    nb, npb = 1 << 20, 1 << 20
+    bk, pkey, pfil, pgrp, pval = config3_inputs(nb, npb, seed=0x5EED0905, key_range=nb + nb // 8)
+    got, info = run_pipeline(ctx, torch_cuda, bk, [pkey, pfil, pgrp, pval], 4096, 499, radix_bits)
+    want, _, _ = po.run_query(bk, pkey, pfil, pgrp, pval, 499)
+    assert got == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want]
+    assert info.rows == nb and info.has_duplicates == 0
+
+
+def test_partitioned_build_of_nothing(ctx, torch_cuda):
+    """A partition op that stores no rows closes its (empty) build; every
+    probe then misses."""
+    bk = np.empty(0, dtype=np.int32)
+    _, pkey, pfil, pgrp, pval = config3_inputs(1 << 12, 1 << 14, seed=0x5EED0906)
+    got, info = run_pipeline(ctx, torch_cuda, bk, [pkey, pfil, pgrp, pval], 4096, 999, 8)
+    assert got == [] and info.rows == 0
+
+
 def test_config3_full_size(ctx, torch_cuda):
     """probe 2^27 rows, build 2^24 keys, 10% selectivity, Zipf(1) over 4096 groups."""
     torch = torch_cuda
