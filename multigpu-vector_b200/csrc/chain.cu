@@ -598,27 +598,41 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* 
     }
 }
 
-// Packs each query's groups into its output region (unsorted) and counts them.
+// Packs each query's groups into its output region (unsorted) and counts them;
+// one warp-aggregated reservation of output rows per warp (a query's counter
+// is one address, and per-row atomics on it serialise in L2).
 __global__ void k_batch_compact(const BatchOut* __restrict__ outs, const BatchItem* __restrict__ items,
                                 uint32_t nitems, uint32_t* err) {
+    const uint32_t lane = lane_id();
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const BatchItem item = items[it];
         const BatchOut& o = outs[item.q];
-        for (uint64_t i = item.lo + threadIdx.x; i < item.hi; i += blockDim.x) {
-            const bool special = i == o.gt.cap;  // one extra index for the group INT32_MIN
-            const int32_t k = special ? kEmptyKey : o.gt.keys[i];
-            const unsigned long long c = special ? o.gt.special[1] : o.gt.counts[i];
-            if ((!special && k == kEmptyKey) || c == 0) continue;
-            const uint32_t pos = atomicAdd(o.count, 1u);
+        // whole warps take part in the ballots
+        const uint64_t end = item.lo + ((item.hi - item.lo + 31) & ~31ull);
+        for (uint64_t i = item.lo + threadIdx.x; i < end; i += blockDim.x) {
+            bool keep = false;
+            mgv_group_row r{};
+            if (i < item.hi) {
+                const bool special = i == o.gt.cap;  // one extra index for the group INT32_MIN
+                const int32_t k = special ? kEmptyKey : o.gt.keys[i];
+                const unsigned long long c = special ? o.gt.special[1] : o.gt.counts[i];
+                keep = (special || k != kEmptyKey) && c != 0;
+                if (keep) {
+                    r.group = k;
+                    r.sum = (int64_t)(special ? o.gt.special[0] : o.gt.sums[i]);
+                    r.count = (int64_t)c;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            uint32_t base = 0;
+            if (lane == 0 && m) base = atomicAdd(o.count, (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!keep) continue;
+            const uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
             if (pos >= o.capacity) {
                 set_error(err, kDevOverflow, 30);
                 continue;
             }
-            mgv_group_row r;
-            r.group = k;
-            r.pad = 0;
-            r.sum = (int64_t)(special ? o.gt.special[0] : o.gt.sums[i]);
-            r.count = (int64_t)c;
             o.rows[pos] = r;
         }
     }
