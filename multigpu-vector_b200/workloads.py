@@ -387,6 +387,7 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
         caps = [tables[t][1] for t, _, _ in reqs]
         offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
         res = np.empty((int(offs[-1]), 3), dtype=np.uint64)  # mgv_group_row = 3 x 64 bits
+        res.fill(0)  # its pages are faulted in here, not by the draining thread while timed
         got = [0] * len(reqs)
         tq: "queue.Queue[tuple[int, int] | None]" = queue.Queue()
         errs = []
