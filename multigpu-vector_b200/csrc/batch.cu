@@ -268,7 +268,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     b->out_rows_total = out_total;
     b->d_qs = reinterpret_cast<ChainDev*>(A + qs_off);
     b->d_jobs = reinterpret_cast<RegionJob*>(A + jobs_off);
-    b->rsc = carve_region_scratch(A + rsc_off, total_regions, build_total, item_regions);
+    b->rsc = carve_region_scratch(A + rsc_off, total_regions, build_total);
     b->total_regions = total_regions;
     b->max_job_regions = max_job_regions;
     b->d_outs = reinterpret_cast<BatchOut*>(A + outs_off);

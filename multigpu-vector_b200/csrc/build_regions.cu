@@ -64,10 +64,8 @@ __device__ __forceinline__ uint32_t region_of(int32_t key, const TableView& t) {
 // Loads of kPrefetch rows per thread are issued before any is used.
 constexpr int kPrefetch = 8;
 
-// Adds the item's rows to the shared per-region counters; lo / hi take the
-// smallest and largest region this thread saw.
-__device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchItem& item, uint32_t* sh,
-                                              uint32_t& lo, uint32_t& hi) {
+// Adds the item's rows to the shared per-region counters.
+__device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchItem& item, uint32_t* sh) {
     for (uint64_t i0 = item.lo + threadIdx.x; i0 < item.hi; i0 += (uint64_t)kRBlock * kPrefetch) {
         int32_t key[kPrefetch];
         bool in[kPrefetch];
@@ -80,12 +78,7 @@ __device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchIt
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u)
-            if (in[u] && key[u] != kEmptyKey) {
-                const uint32_t r = region_of(key[u], sj.t);
-                atomicAdd(sh + r, 1u);
-                lo = min(lo, r);
-                hi = max(hi, r);
-            }
+            if (in[u] && key[u] != kEmptyKey) atomicAdd(sh + region_of(key[u], sj.t), 1u);
     }
 }
 
@@ -112,8 +105,7 @@ __global__ void __launch_bounds__(kRBlock) k_region_hist(const RegionJob* __rest
         }
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) sh[r] = 0;
         __syncthreads();
-        uint32_t lo = ~0u, hi = 0;
-        count_regions(sj, item, sh, lo, hi);
+        count_regions(sj, item, sh);
         __syncthreads();
         const uint64_t base = item_ioff(items, item, it, sj.nregions);
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock)
@@ -533,7 +525,7 @@ size_t region_scratch_bytes(uint32_t regions, uint64_t rows, uint64_t item_regio
            a(4ull * item_regions);
 }
 
-RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows, uint64_t item_regions) {
+RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows) {
     auto a = [](size_t x) { return (x + 255) & ~(size_t)255; };
     unsigned char* p = static_cast<unsigned char*>(base);
     RegionScratch s;
@@ -549,8 +541,7 @@ RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows, 
     p += a(8ull * rows);
     s.ovf = reinterpret_cast<unsigned long long*>(p);
     p += a(8ull * rows);
-    s.ioff = reinterpret_cast<uint32_t*>(p);
-    (void)item_regions;
+    s.ioff = reinterpret_cast<uint32_t*>(p);  // item_regions entries, the last part
     return s;
 }
 

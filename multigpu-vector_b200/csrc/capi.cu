@@ -1093,7 +1093,7 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
             }
             const RegionJob job{term->table, cols[kc], pays, filt, bound, 0, regions, 0};
             MGV_CUDA_TRY(launch_build_regions(nullptr, job, 1, nullptr, 0, n, rows_per_item, regions, regions,
-                                              carve_region_scratch(term->rb_scratch, regions, n, item_regions), fresh,
+                                              carve_region_scratch(term->rb_scratch, regions, n), fresh,
                                               term->hb_partitioned && !sel, s, ctx));
             return MGV_OK;
         }

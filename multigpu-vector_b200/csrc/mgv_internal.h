@@ -294,7 +294,7 @@ struct RegionScratch {
 void sort_group_rows(std::vector<mgv_group_row>& v);
 inline uint32_t table_regions(const TableView& t) { return (t.nbuckets + kRegionBuckets - 1) / kRegionBuckets; }
 size_t region_scratch_bytes(uint32_t regions, uint64_t rows, uint64_t item_regions);
-RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows, uint64_t item_regions);
+RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows);
 // Items: explicit (job, rows) items, or (items == nullptr) rows [0, n) of
 // job0 cut into items of rows_per_item.  fresh: the tables hold nothing yet
 // and are not cleared beforehand; every region is written.  partitioned
