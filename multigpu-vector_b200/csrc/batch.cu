@@ -219,27 +219,18 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         delete b;
         return fail(MGV_EUNSUPPORTED, "a batch holds fewer than 2^31 build rows");
     }
-    // work items; a build item's aux is its first entry of the per-(item, region) offsets
+    const size_t rsc_off = take(region_scratch_bytes(total_regions, build_total));
+    const size_t outs_off = take(sizeof(BatchOut) * std::max(nq, 1u));
+    // work items
     std::vector<BatchItem> bi, pi, ci;
-    uint64_t item_regions = 0;
     for (uint32_t i = 0; i < nq; ++i) {
-        const uint32_t qregions = (nbk[i] + kRegionBuckets - 1) / kRegionBuckets;
-        for (uint64_t lo = 0; lo < qs[i].build_rows; lo += cfg.build_item_rows) {
-            if (item_regions + qregions >= (1ull << 32)) {
-                delete b;
-                return fail(MGV_EUNSUPPORTED, "a batch's build items span too many table regions");
-            }
-            bi.push_back(BatchItem{i, (uint32_t)item_regions, lo,
-                                   std::min<uint64_t>(qs[i].build_rows, lo + cfg.build_item_rows)});
-            item_regions += qregions;
-        }
+        for (uint64_t lo = 0; lo < qs[i].build_rows; lo += cfg.build_item_rows)
+            bi.push_back(BatchItem{i, 0, lo, std::min<uint64_t>(qs[i].build_rows, lo + cfg.build_item_rows)});
         for (uint64_t lo = 0; lo < qs[i].probe_rows; lo += cfg.probe_item_rows)
             pi.push_back(BatchItem{i, 0, lo, std::min<uint64_t>(qs[i].probe_rows, lo + cfg.probe_item_rows)});
         for (uint64_t lo = 0; lo <= gcap[i]; lo += 65536)
             ci.push_back(BatchItem{i, 0, lo, std::min<uint64_t>((uint64_t)gcap[i] + 1, lo + 65536)});
     }
-    const size_t rsc_off = take(region_scratch_bytes(total_regions, build_total, item_regions));
-    const size_t outs_off = take(sizeof(BatchOut) * std::max(nq, 1u));
     const size_t bi_off = take(sizeof(BatchItem) * std::max<size_t>(bi.size(), 1));
     const size_t pi_off = take(sizeof(BatchItem) * std::max<size_t>(pi.size(), 1));
     const size_t ci_off = take(sizeof(BatchItem) * std::max<size_t>(ci.size(), 1));

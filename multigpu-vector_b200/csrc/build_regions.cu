@@ -5,14 +5,11 @@
 // B200 even with the table in L2, and slower with more rows in flight).  Here
 // the table is cut into regions of kRegionBuckets buckets (64 KiB) and built
 // region by region in shared memory:
-//   1. k_region_hist     rows per region (per-CTA shared histogram per item);
-//                        the atomicAdd that adds an item's count to a region's
-//                        total returns the item's offset in that region, kept
-//                        per (item, region)
+//   1. k_region_hist     rows per region (per-CTA shared histogram per item)
 //   2. k_region_scan     exclusive prefix sum -> each region's staging range
 //   3. k_region_scatter  every row, packed {key, payload}, to its region's
-//                        range (per item: shared-memory cursors that start at
-//                        the region's start + the item's offset)
+//                        range (per item: one global reservation per region,
+//                        then shared-memory cursors)
 //   4. k_region_build    one CTA per region: the region is loaded into shared
 //                        memory (or starts empty), each row claims a slot
 //                        with one shared atomicAdd on its bucket's fill
@@ -51,7 +48,7 @@ __device__ __forceinline__ BatchItem item_at(const BatchItem* items, uint32_t it
     if (items) return items[it];
     BatchItem b;
     b.q = 0;
-    b.aux = 0;
+    b.pad = 0;
     b.lo = (uint64_t)it * rpi;
     b.hi = min(n, b.lo + rpi);
     return b;
@@ -82,16 +79,9 @@ __device__ __forceinline__ void count_regions(const RegionJob& sj, const BatchIt
     }
 }
 
-// The first entry of RegionScratch::ioff for item `it`.
-__device__ __forceinline__ uint64_t item_ioff(const BatchItem* items, const BatchItem& item, uint32_t it,
-                                              uint32_t nregions) {
-    return items ? (uint64_t)item.aux : (uint64_t)it * nregions;
-}
-
 __global__ void __launch_bounds__(kRBlock) k_region_hist(const RegionJob* __restrict__ jobs, RegionJob job0,
                                                          const BatchItem* __restrict__ items, uint32_t nitems,
-                                                         uint64_t n, uint64_t rpi, uint32_t* __restrict__ hist,
-                                                         uint32_t* __restrict__ ioff) {
+                                                         uint64_t n, uint64_t rpi, uint32_t* __restrict__ hist) {
     extern __shared__ uint32_t sh[];
     __shared__ RegionJob sj;
     int64_t cur = -1;
@@ -107,9 +97,8 @@ __global__ void __launch_bounds__(kRBlock) k_region_hist(const RegionJob* __rest
         __syncthreads();
         count_regions(sj, item, sh);
         __syncthreads();
-        const uint64_t base = item_ioff(items, item, it, sj.nregions);
         for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock)
-            if (sh[r]) ioff[base + r] = atomicAdd(hist + sj.region0 + r, sh[r]);
+            if (sh[r]) atomicAdd(hist + sj.region0 + r, sh[r]);
     }
 }
 
@@ -140,8 +129,7 @@ __global__ void __launch_bounds__(kScanBlock) k_region_scan(const uint32_t* __re
 
 __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __restrict__ jobs, RegionJob job0,
                                                             const BatchItem* __restrict__ items, uint32_t nitems,
-                                                            uint64_t n, uint64_t rpi, const uint32_t* __restrict__ start,
-                                                            const uint32_t* __restrict__ ioff,
+                                                            uint64_t n, uint64_t rpi, uint32_t* __restrict__ cursor,
                                                             unsigned long long* __restrict__ staging, uint32_t* err) {
     extern __shared__ uint32_t sh[];
     __shared__ RegionJob sj;
@@ -154,10 +142,15 @@ __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __r
             cur = item.q;
             __syncthreads();
         }
-        // the item's cursors: region start + the item's offset in the region
-        // (entries of regions the item has no rows in are never used)
-        const uint64_t base = item_ioff(items, item, it, sj.nregions);
-        for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) sh[r] = start[sj.region0 + r] + ioff[base + r];
+        for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) sh[r] = 0;
+        __syncthreads();
+        count_regions(sj, item, sh);
+        __syncthreads();
+        // one reservation per region and item; sh[r] becomes the region's next staging row
+        for (uint32_t r = threadIdx.x; r < sj.nregions; r += kRBlock) {
+            const uint32_t c = sh[r];
+            if (c) sh[r] = atomicAdd(cursor + sj.region0 + r, c);
+        }
         __syncthreads();
         for (uint64_t i0 = item.lo + threadIdx.x; i0 < item.hi; i0 += (uint64_t)kRBlock * kPrefetch) {
             int32_t key[kPrefetch], pay[kPrefetch];
@@ -519,10 +512,9 @@ __global__ void k_region_overflow(const RegionJob* __restrict__ jobs, RegionJob 
 
 }  // namespace
 
-size_t region_scratch_bytes(uint32_t regions, uint64_t rows, uint64_t item_regions) {
+size_t region_scratch_bytes(uint32_t regions, uint64_t rows) {
     auto a = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    return a(4ull * regions) + a(4ull * (regions + 1)) + a(4ull * regions) + a(4) + a(8ull * rows) + a(8ull * rows) +
-           a(4ull * item_regions);
+    return a(4ull * regions) + a(4ull * (regions + 1)) + a(4ull * regions) + a(4) + a(8ull * rows) + a(8ull * rows);
 }
 
 RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows) {
@@ -540,8 +532,6 @@ RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows) 
     s.staging = reinterpret_cast<unsigned long long*>(p);
     p += a(8ull * rows);
     s.ovf = reinterpret_cast<unsigned long long*>(p);
-    p += a(8ull * rows);
-    s.ioff = reinterpret_cast<uint32_t*>(p);  // item_regions entries, the last part
     return s;
 }
 
@@ -568,7 +558,7 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
     if (nitems) {
         const int grid = (int)std::min<uint64_t>(nitems, (uint64_t)occupancy_grid((const void*)k_region_hist, kRBlock,
                                                                                    hsmem, ctx));
-        k_region_hist<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.hist, sc.ioff);
+        k_region_hist<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.hist);
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     }
@@ -586,8 +576,8 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
     } else if (nitems) {
         const int grid = (int)std::min<uint64_t>(
             nitems, (uint64_t)occupancy_grid((const void*)k_region_scatter, kRBlock, hsmem, ctx));
-        k_region_scatter<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.start,
-                                                      sc.ioff, sc.staging, ctx->d_err);
+        k_region_scatter<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.cursor,
+                                                      sc.staging, ctx->d_err);
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     }

@@ -1076,11 +1076,7 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
                 return MGV_OK;
             }
             // shared-memory build; its scratch is kept by the operator and grown on demand
-            // items: two per SM, each worth zeroing and flushing its region histogram
-            const uint64_t rows_per_item =
-                std::max<uint64_t>({8ull * regions, 4096, n / (2ull * ctx->prop.multiProcessorCount) + 1});
-            const uint64_t item_regions = (n + rows_per_item - 1) / rows_per_item * regions;
-            const size_t need = region_scratch_bytes(regions, n, item_regions);
+            const size_t need = region_scratch_bytes(regions, n);
             if (term->rb_bytes < need) {
                 if (term->rb_scratch) {
                     MGV_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1092,6 +1088,9 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
                 term->rb_bytes = need;
             }
             const RegionJob job{term->table, cols[kc], pays, filt, bound, 0, regions, 0};
+            // items: two per SM, each worth zeroing and flushing its region histogram
+            const uint64_t rows_per_item =
+                std::max<uint64_t>({8ull * regions, 4096, n / (2ull * ctx->prop.multiProcessorCount) + 1});
             MGV_CUDA_TRY(launch_build_regions(nullptr, job, 1, nullptr, 0, n, rows_per_item, regions, regions,
                                               carve_region_scratch(term->rb_scratch, regions, n), fresh,
                                               term->hb_partitioned && !sel, s, ctx));

@@ -258,7 +258,7 @@ constexpr int32_t kBP = 100;  // terminal reference to the build payload
 // Batched execution (chain.cu kernels, batch.cu host side).
 struct BatchItem {  // rows [lo, hi) of query q
     uint32_t q;
-    uint32_t aux;  // build items: the item's first entry of RegionScratch::ioff; 0 otherwise
+    uint32_t pad;
     uint64_t lo, hi;
 };
 // Shared-memory hash-table build (build_regions.cu).  A table is cut into
@@ -287,13 +287,11 @@ struct RegionScratch {
     uint32_t* ovf_count;      // [1]
     unsigned long long* staging;  // [rows] {key, payload}, region-major
     unsigned long long* ovf;  // [rows] job << 32 | staging row, left for the global insert
-    uint32_t* ioff;           // per (item, region of its job): the item's first row in the region,
-                              // relative to the region's start (written by the histogram pass)
 };
 // Host: group rows in ascending group order (radix sort).
 void sort_group_rows(std::vector<mgv_group_row>& v);
 inline uint32_t table_regions(const TableView& t) { return (t.nbuckets + kRegionBuckets - 1) / kRegionBuckets; }
-size_t region_scratch_bytes(uint32_t regions, uint64_t rows, uint64_t item_regions);
+size_t region_scratch_bytes(uint32_t regions, uint64_t rows);
 RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows);
 // Items: explicit (job, rows) items, or (items == nullptr) rows [0, n) of
 // job0 cut into items of rows_per_item.  fresh: the tables hold nothing yet
