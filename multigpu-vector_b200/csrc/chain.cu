@@ -229,45 +229,6 @@ __device__ __forceinline__ void group_add_row(const SmemGroups& sg, const GroupT
     global_group_add(gt, g, (unsigned long long)(long long)v, 1ull, err);
 }
 
-// Up to four rows (g[j], v[j], active when act[j]) of one lane at once: the
-// home slots of all four are read together, then the shared atomics of all
-// rows found there are issued together, so the lane waits about two shared
-// round trips for the four instead of two per row.  A row whose group is not
-// at its home slot (a new group or a collision) takes group_add_row.
-__device__ __forceinline__ void group_add_rows4(const SmemGroups& sg, const GroupTableView& gt, const int32_t (&g)[4],
-                                                const int32_t (&v)[4], const bool (&act)[4], uint32_t* err) {
-    uint32_t slot[4];
-    bool hit[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        hit[j] = false;
-        slot[j] = sg.cap;  // the reserved group's slot
-        if (!act[j] || !sg.cap) continue;
-        if (g[j] == kEmptyKey) {
-            hit[j] = true;
-        } else {
-            slot[j] = group_hash(g[j], sg.cap);
-            hit[j] = *((volatile int32_t*)(sg.keys + slot[j])) == g[j];
-        }
-    }
-    uint32_t x[4], old[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-        if (hit[j]) {
-            x[j] = (uint32_t)v[j] ^ 0x80000000u;  // v + 2^31
-            atomicAdd(sg.cnt + slot[j], 1u);
-            old[j] = atomicAdd(sg.lo + slot[j], x[j]);
-        }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (hit[j]) {
-            if (old[j] + x[j] < old[j]) atomicAdd(sg.hi + slot[j], 1u);
-        } else if (act[j]) {
-            group_add_row(sg, gt, g[j], v[j], err);
-        }
-    }
-}
-
 __device__ __forceinline__ void smem_groups_init(const SmemGroups& sg) {
     for (uint32_t i = threadIdx.x; i <= sg.cap; i += blockDim.x) {
         sg.keys[i] = kEmptyKey;
@@ -431,8 +392,6 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                 }
             }
             for (uint32_t round = 0; round <= nbuckets; ++round) {
-                bool gf[4] = {false, false, false, false};
-                int32_t gbp[4] = {0, 0, 0, 0};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const uint32_t k = (uint32_t)key[j];
@@ -445,12 +404,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                                 f = true;
                                 bp = (int32_t)w[j][2 * q + 1];
                             }
-                        if (TERM == kTermGroupby) {  // the four rows go to the group table together, below
-                            gf[j] = f;
-                            gbp[j] = bp;
-                        } else if (__any_sync(0xffffffffu, f)) {
-                            emit(f, j, bp);
-                        }
+                        if (__any_sync(0xffffffffu, f)) emit(f, j, bp);
                         live[j] = live[j] && !f && w[j][6] != (uint32_t)kEmptyKey;
                     } else {  // every match of the run
 #pragma unroll
@@ -460,15 +414,6 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                         }
                         live[j] = live[j] && w[j][6] != (uint32_t)kEmptyKey;
                     }
-                }
-                if (TERM == kTermGroupby && unique && __any_sync(0xffffffffu, gf[0] || gf[1] || gf[2] || gf[3])) {
-                    int32_t gg[4], gx[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        gg[j] = val(ref0, j, gbp[j]);
-                        gx[j] = ref1 >= 0 ? val(ref1, j, gbp[j]) : 0;
-                    }
-                    group_add_rows4(sg, a.gt, gg, gx, gf, err);
                 }
                 if (!__any_sync(0xffffffffu, live[0] || live[1] || live[2] || live[3])) break;
 #pragma unroll
