@@ -463,9 +463,10 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
             return st;
         }
     }
-    // landing zones pinned up front, so serving rarely pins (slow) while
-    // batches are in flight and waiters still hold earlier zones
-    for (uint32_t i = 0; i < 4 * S->cfg.max_inflight; ++i) {
+    // landing zones pinned up front (four per in-flight slot, at most eight),
+    // so serving rarely pins (slow) while batches are in flight and waiters
+    // still hold earlier zones
+    for (uint32_t i = 0; i < std::min(4 * S->cfg.max_inflight, 8u); ++i) {
         auto L = std::make_unique<Landing>();
         L->cap = kMinLandingRows;
         L->ncounts = S->cfg.max_batch;
