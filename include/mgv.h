@@ -241,8 +241,9 @@ typedef struct mgv_group_row {
 /* split (src/operators/split.cu:49-118, partition by x & 1), generalised to
  * 2^radix_bits partitions by (cols[key_col] >> radix_shift) & (2^bits - 1):
  * the in-GPU exchange.  Rows are stored partition-major (capacity
- * max_rows); close() pushes them, partition by partition, into the parent
- * chain and then closes it. */
+ * max_rows; a consume does not wait for the device); close() pushes them
+ * into the parent chain and then closes it.  Rows past max_rows are dropped
+ * and close() returns MGV_ENOMEM. */
 typedef struct mgv_partition_desc {
     uint32_t key_col;
     uint32_t radix_bits;
