@@ -9,7 +9,10 @@
 //   2. k_region_scan     exclusive prefix sum -> each region's staging range
 //   3. k_region_scatter  every row, packed {key, payload}, to its region's
 //                        range (per item: one global reservation per region,
-//                        then shared-memory cursors)
+//                        then shared-memory cursors); for input already
+//                        partitioned on the table's radix bits,
+//                        k_region_scatter_sorted instead: each warp sorts its
+//                        256-row tile by region and stores runs
 //   4. k_region_build    one CTA per region: the region is loaded into shared
 //                        memory (or starts empty), each row claims a slot
 //                        with one shared atomicAdd on its bucket's fill
