@@ -143,6 +143,26 @@ mgv_status mgv_pool_register_producer(mgv_pool *pool);
 mgv_status mgv_pool_unregister_producer(mgv_pool *pool);
 mgv_status mgv_pool_stats_get(mgv_pool *pool, mgv_pool_stats *out);
 
+/* Device view of a pool for kernels that acquire and release buffers
+ * themselves (include/mgv_device.cuh: mgv_dev_buffer_acquire /
+ * mgv_dev_buffer_release, the device-side get_buffer / release_buffer of
+ * src/buffer_manager.cuh:50-64,96-129).  Every pointer is a device address. */
+typedef struct mgv_pool_device {
+    unsigned long long *head;  /* free stack head: {top id, tag}              */
+    uint32_t *available;       /* buffers on the free stack                   */
+    uint32_t *producers;       /* registered producers                        */
+    uint32_t *next;            /* [nbuffers] free-stack links                 */
+    int32_t *slab;             /* buffer i, column c at slab + (i*ncols + c)*capacity */
+    uint32_t nbuffers;
+    uint32_t capacity;
+    uint32_t ncols;
+    uint32_t reserved;
+} mgv_pool_device;
+
+/* Fills *out with the pool's device view (buffer_manager's __constant__ pool
+ * pointer, src/buffer_manager.cuh:40-48, handed to kernels explicitly). */
+mgv_status mgv_pool_device_get(mgv_pool *pool, mgv_pool_device *out);
+
 /* ---- operators -------------------------------------------------------- */
 /*
  * Operators form push chains as in the reference (d_operator_t with a
@@ -459,33 +479,26 @@ mgv_status mgv_server_destroy(mgv_server *s);
 #define MGV_NOALLOC_MAX_BUILD_ROWS (1u << 20)
 
 /* No counterpart in the reference.  For callers that cannot allocate device
- * memory (code running under another framework's allocator or memory
- * budget, inside a graph capture or real-time loop where an allocation would
- * stall, or given only pre-allocated buffers): builds a hash table on the
- * build columns and probes it with the probe columns, writing
- * d_result[0] = COUNT(matches) and d_result[1] = SUM(build payload + probe
- * payload) (int64, device memory) -- the result of
- * create_count_join_1G_pipeline.  Needs no context and allocates nothing:
- * the table lives in a fixed device array of MGV_NOALLOC_MAX_BUILD_ROWS rows
- * (about 20 MiB, held by every GPU that loads the library until exit); a
- * larger build side is rejected with MGV_EINVAL.  The first call on a device
- * looks up the array's device address and should come before any stream
- * capture.  All calls share the array and clear it first: calls that overlap
- * on the GPU race.  Payload pointers may be NULL (payload 0).  Waits for
- * `stream` before returning. */
+ * memory: code running under another framework's allocator or memory budget
+ * (which owns every byte and forbids cudaMalloc), plugins and embedded hosts
+ * that are handed only pre-allocated buffers, and processes whose device
+ * memory is already spoken for.  Builds a hash table on the build columns and
+ * probes it with the probe columns, writing d_result[0] = COUNT(matches) and
+ * d_result[1] = SUM(build payload + probe payload) (int64, device memory) --
+ * the result of create_count_join_1G_pipeline.  Needs no context and
+ * allocates nothing: the table lives in a fixed file-scope device array of
+ * MGV_NOALLOC_MAX_BUILD_ROWS rows (about 20 MiB per device, committed by the
+ * first call on that device -- or at module load under
+ * CUDA_MODULE_LOADING=EAGER -- and held until the process exits); a larger
+ * build side is rejected with MGV_EINVAL.  The first call on a device looks
+ * up the array's device address and should come before any stream capture.
+ * All calls share the array and clear it first: calls that overlap on the
+ * GPU race.  Payload pointers may be NULL (payload 0).  Runs with `device`
+ * current and restores the caller's current device; waits for `stream`
+ * before returning. */
 mgv_status mgv_hash_join_noalloc(int device, const int32_t *build_keys, const int32_t *build_payloads,
                                  uint64_t build_rows, const int32_t *probe_keys, const int32_t *probe_payloads,
                                  uint64_t probe_rows, int64_t *d_result, void *stream);
-
-/* ---- diagnostics ------------------------------------------------------ */
-
-/* Random 32-byte bucket-read ceiling: times `reps` passes of n hashed
- * 32-byte loads into a table of table_bytes (R = 4 loads in flight per
- * thread, ctas_per_sm CTAs of 256 threads per SM) and returns the mean
- * milliseconds per pass.  The bound every hash probe is measured against;
- * no reference counterpart. */
-mgv_status mgv_diag_random_gather(mgv_ctx *ctx, uint64_t table_bytes, uint64_t n, uint32_t ctas_per_sm,
-                                  uint32_t reps, double *ms_per_pass);
 
 #ifdef __cplusplus
 }

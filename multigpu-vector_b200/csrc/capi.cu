@@ -445,6 +445,20 @@ mgv_status mgv_pool_stats_get(mgv_pool* p, mgv_pool_stats* out) {
     return MGV_OK;
 }
 
+mgv_status mgv_pool_device_get(mgv_pool* p, mgv_pool_device* out) {
+    if (!p || !out) return fail(MGV_EINVAL, "NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    out->head = &p->dev->head;
+    out->available = &p->dev->available;
+    out->producers = &p->dev->producers;
+    out->next = p->dev->next;
+    out->slab = p->slab;
+    out->nbuffers = p->nbuffers;
+    out->capacity = p->capacity;
+    out->ncols = p->ncols;
+    return MGV_OK;
+}
+
 // ---- operators -------------------------------------------------------------
 
 static mgv_op* new_op(Context* ctx, OpKind k) {

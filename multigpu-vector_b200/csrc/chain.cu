@@ -22,6 +22,7 @@
 // table; at the end of the CTA the shared table is merged into the global one.
 #include <cuda_runtime.h>
 
+#include "../../include/mgv_device.cuh"
 #include "device_common.cuh"
 #include "hash_table.cuh"
 #include "mgv_internal.h"
@@ -40,19 +41,15 @@ constexpr size_t kRingBytes = (size_t)kChainWarps * kIdRing * sizeof(uint32_t);
 
 // ---- device buffer pool: pop (swap-on-full for the sink) -------------------
 
-__device__ __forceinline__ uint32_t pool_pop(PoolDev* p, uint32_t tries) {
-    for (uint32_t i = 0; i < tries; ++i) {
-        unsigned long long h = atomicAdd(&p->head, 0ull);
-        uint32_t top = (uint32_t)h;
-        if (top == kNil) return kNil;
-        uint32_t nxt = *((volatile uint32_t*)&p->next[top]);
-        unsigned long long nh = (((h >> 32) + 1ull) << 32) | nxt;
-        if (atomicCAS(&p->head, h, nh) == h) {
-            atomicSub(&p->available, 1u);
-            return top;
-        }
-    }
-    return kNil;
+// One pop from the pool's device free stack (include/mgv_device.cuh), or kNil.
+__device__ __forceinline__ uint32_t pool_pop(PoolDev* p) {
+    mgv_pool_device v;
+    v.head = &p->head;
+    v.available = &p->available;
+    v.producers = &p->producers;
+    v.next = p->next;
+    uint32_t id;
+    return mgv_dev_stack_pop(&v, &id) ? id : kNil;
 }
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -66,7 +63,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // a bounded wait (swap-on-full, src/buffer_manager.cuh:147-176).
 __device__ uint32_t sink_chunk(const SinkView& s, uint32_t c, bool opener, uint32_t* err) {
     if (opener) {
-        uint32_t id = pool_pop(s.pool, 4096);
+        uint32_t id = pool_pop(s.pool);
         if (id == kNil) {
             set_error(err, kDevOverflow, 3);
             id = kNil - 1;  // published "no buffer" marker

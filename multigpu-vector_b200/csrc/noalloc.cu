@@ -2,22 +2,24 @@
 //
 // Some callers cannot allocate device memory: code that runs inside another
 // framework's memory budget or allocator (which owns every byte and forbids
-// cudaMalloc), callers inside a CUDA-graph capture or a real-time loop where
-// an allocation would synchronise or stall, and embedded hosts that are only
-// handed pre-allocated buffers.  They cannot create a context or a
-// hash_build operator, because both allocate.  mgv_hash_join_noalloc gives
-// them the join of create_count_join_1G_pipeline -- build, then probe, then
-// COUNT(matches) and SUM(build payload + probe payload) -- with its hash table
-// in a file-scope device array instead of allocated memory.
+// cudaMalloc), plugins and embedded hosts that are only handed
+// pre-allocated buffers, and processes whose device memory is already spoken
+// for.  They cannot create a context or a hash_build operator, because both
+// allocate.  mgv_hash_join_noalloc gives them the join of
+// create_count_join_1G_pipeline -- build, then probe, then COUNT(matches) and
+// SUM(build payload + probe payload) -- with its hash table in a file-scope
+// device array instead of allocated memory.
 //
 // The array is fixed at MGV_NOALLOC_MAX_BUILD_ROWS build rows (a 16 MiB
-// table at load factor 0.5 plus a 4 MiB side list for INT32_MIN keys); every
-// GPU that loads the library holds it until the process exits.  Host code
-// cannot use the array's name as a device address, so each device's address
-// is looked up once with cudaGetSymbolAddress (with that device current) by
-// the first call on that device.  All calls share the array and each call
-// clears it, so calls that overlap on the GPU (other threads, other streams)
-// race and must be serialised by the caller.
+// table at load factor 0.5 plus a 4 MiB side list for INT32_MIN keys).  With
+// lazy module loading (the CUDA default) a device commits it when the first
+// call on that device looks up its address, or when the module loads under
+// CUDA_MODULE_LOADING=EAGER; it is then held until the process exits.  Host
+// code cannot use the array's name as a device address, so each device's
+// address is looked up once with cudaGetSymbolAddress (with that device
+// current) by the first call on that device.  All calls share the array and
+// each call clears it, so calls that overlap on the GPU (other threads,
+// other streams) race and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -71,6 +73,10 @@ mgv_status setup(int device, DeviceSlot*& out) {
     return MGV_OK;
 }
 
+mgv_status join_on_device(int device, const int32_t* build_keys, const int32_t* build_payloads, uint64_t build_rows,
+                          const int32_t* probe_keys, const int32_t* probe_payloads, uint64_t probe_rows,
+                          int64_t* d_result, void* stream);
+
 }  // namespace
 }  // namespace mgv
 
@@ -89,7 +95,27 @@ extern "C" mgv_status mgv_hash_join_noalloc(int device, const int32_t* build_key
     int ndev = 0;
     MGV_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev || device >= kMaxDevices) return fail(MGV_EINVAL, "no such device");
+    // The join runs with `device` current; the caller's current device is
+    // restored on every return path.
+    int caller_device = 0;
+    MGV_CUDA_TRY(cudaGetDevice(&caller_device));
+    if (caller_device == device) return join_on_device(device, build_keys, build_payloads, build_rows, probe_keys,
+                                                       probe_payloads, probe_rows, d_result, stream);
     MGV_CUDA_TRY(cudaSetDevice(device));
+    const mgv_status st = join_on_device(device, build_keys, build_payloads, build_rows, probe_keys, probe_payloads,
+                                         probe_rows, d_result, stream);
+    const cudaError_t back = cudaSetDevice(caller_device);
+    if (st == MGV_OK && back != cudaSuccess) return cuda_fail(back, "cudaSetDevice(caller's device)");
+    return st;
+}
+
+namespace mgv {
+namespace {
+
+// The join itself, with `device` current.
+mgv_status join_on_device(int device, const int32_t* build_keys, const int32_t* build_payloads, uint64_t build_rows,
+                          const int32_t* probe_keys, const int32_t* probe_payloads, uint64_t probe_rows,
+                          int64_t* d_result, void* stream) {
     DeviceSlot* slot = nullptr;
     mgv_status st = setup(device, slot);
     if (st != MGV_OK) return st;
@@ -133,3 +159,6 @@ extern "C" mgv_status mgv_hash_join_noalloc(int device, const int32_t* build_key
     }
     return MGV_OK;
 }
+
+}  // namespace
+}  // namespace mgv

@@ -13,47 +13,26 @@
 // src/lockfree_stack.cuh:122, src/threadsafe_device_stack.cuh:48).
 #include <cuda_runtime.h>
 
+#include "../../include/mgv_device.cuh"
 #include "device_common.cuh"
 #include "mgv_internal.h"
 
 namespace mgv {
 
-__device__ __forceinline__ unsigned long long pool_now_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Tagged Treiber stack (the tag in the high word defeats ABA, as the
-// reference's tagged_uint32_t does, src/lockfree_stack.cuh:21-67).
-__device__ bool stack_pop(PoolDev* p, uint32_t* out) {
-    for (int i = 0; i < 4096; ++i) {
-        unsigned long long h = atomicAdd(&p->head, 0ull);
-        uint32_t top = (uint32_t)h;
-        if (top == kNil) return false;
-        uint32_t nxt = *((volatile uint32_t*)&p->next[top]);
-        unsigned long long nh = (((h >> 32) + 1ull) << 32) | nxt;
-        if (atomicCAS(&p->head, h, nh) == h) {
-            atomicSub(&p->available, 1u);
-            *out = top;
-            return true;
-        }
-    }
-    return false;
-}
-
-__device__ bool stack_push(PoolDev* p, uint32_t id) {
-    for (int i = 0; i < 4096; ++i) {
-        unsigned long long h = atomicAdd(&p->head, 0ull);
-        *((volatile uint32_t*)&p->next[id]) = (uint32_t)h;
-        __threadfence();
-        unsigned long long nh = (((h >> 32) + 1ull) << 32) | id;
-        if (atomicCAS(&p->head, h, nh) == h) {
-            atomicAdd(&p->available, 1u);
-            return true;
-        }
-    }
-    return false;
+// The device view of a pool, the form the public device header's stack
+// operations take (one implementation for the library and for user kernels).
+__device__ __forceinline__ mgv_pool_device pool_view(PoolDev* p) {
+    mgv_pool_device v;
+    v.head = &p->head;
+    v.available = &p->available;
+    v.producers = &p->producers;
+    v.next = p->next;
+    v.slab = nullptr;
+    v.nbuffers = p->nbuffers;
+    v.capacity = 0;
+    v.ncols = 0;
+    v.reserved = 0;
+    return v;
 }
 
 __global__ void k_pool_init(PoolDev* p, uint32_t n) {
@@ -73,10 +52,11 @@ __global__ void k_pool_pop_batch(PoolDev* p, uint32_t want, uint64_t timeout_ns,
                                  uint32_t* got_status) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     uint32_t got = 0, status = 0;
-    const unsigned long long t0 = pool_now_ns();
+    const mgv_pool_device v = pool_view(p);
+    const unsigned long long t0 = mgv_dev_now_ns();
     while (got < want) {
         uint32_t id;
-        if (stack_pop(p, &id)) {
+        if (mgv_dev_stack_pop(&v, &id)) {
             out[got++] = id;
             continue;
         }
@@ -85,7 +65,7 @@ __global__ void k_pool_pop_batch(PoolDev* p, uint32_t want, uint64_t timeout_ns,
             status = 2;
             break;
         }
-        if (pool_now_ns() - t0 >= timeout_ns) {
+        if (mgv_dev_now_ns() - t0 >= timeout_ns) {
             status = 1;
             break;
         }
@@ -97,8 +77,9 @@ __global__ void k_pool_pop_batch(PoolDev* p, uint32_t want, uint64_t timeout_ns,
 
 __global__ void k_pool_push_batch(PoolDev* p, const uint32_t* ids, uint32_t n, uint32_t* err) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const mgv_pool_device v = pool_view(p);
     for (uint32_t i = 0; i < n; ++i)
-        if (!stack_push(p, ids[i])) set_error(err, kDevTimeout, 7);
+        if (!mgv_dev_stack_push(&v, ids[i])) set_error(err, kDevTimeout, 7);
 }
 
 __global__ void k_pool_producers(PoolDev* p, int delta) {

@@ -17,7 +17,10 @@ from ctypes import c_uint32, c_uint64, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmgv.so")
-HEADER = os.path.join(os.path.dirname(HERE), "include", "mgv.h")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+HEADER = os.path.join(INCLUDE, "mgv.h")
+# Every public header: the operator API (mgv.h) and the diagnostics (mgv_diag.h).
+HEADERS = [os.path.join(INCLUDE, f) for f in ("mgv.h", "mgv_diag.h")]
 
 MAX_COLS = 8
 # Rows per pool buffer by default (DEFAULT_BUFF_CAP, src/common.cuh:8-10).
@@ -59,6 +62,12 @@ class PoolStats(ctypes.Structure):
     _fields_ = [("nbuffers", c_uint32), ("capacity", c_uint32), ("ncols", c_uint32),
                 ("available", c_uint32), ("host_cached", c_uint32), ("producers", c_uint32),
                 ("bytes", c_uint64)]
+
+
+class PoolDevice(ctypes.Structure):
+    _fields_ = [("head", c_void_p), ("available", c_void_p), ("producers", c_void_p), ("next", c_void_p),
+                ("slab", c_void_p), ("nbuffers", c_uint32), ("capacity", c_uint32), ("ncols", c_uint32),
+                ("reserved", c_uint32)]
 
 
 class SelectDesc(ctypes.Structure):
@@ -137,6 +146,12 @@ class ServerStats(ctypes.Structure):
                 ("solo", c_uint64)]
 
 
+class DiagGatherDesc(ctypes.Structure):
+    _fields_ = [("table_bytes", c_uint64), ("lookups", c_uint64), ("line_bytes", c_uint32), ("method", c_uint32),
+                ("ctas_per_sm", c_uint32), ("reps", c_uint32), ("inflight", c_uint32), ("lsu_warps", c_uint32),
+                ("tma_warps", c_uint32), ("tma_share", c_float)]
+
+
 class SinkDesc(ctypes.Structure):
     _fields_ = [("pool", c_void_p), ("max_buffers", c_uint32), ("reserved", c_uint32)]
 
@@ -144,11 +159,14 @@ class SinkDesc(ctypes.Structure):
 _lib = None
 
 
-def header_functions(path: str = HEADER) -> list[str]:
-    """Names of the functions include/mgv.h declares."""
-    text = open(path).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(mgv_[a-z0-9_]+)\s*\(", text)))
+def header_functions(paths=None) -> list[str]:
+    """Names of the functions the public headers (include/*.h) declare."""
+    names = set()
+    for path in paths or HEADERS:
+        text = open(path).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\b(mgv_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def load(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -216,6 +234,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "mgv_hash_join_noalloc": (st, [c_int, c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_uint64,
                                        c_void_p, c_void_p]),
         "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
+        "mgv_pool_device_get": (st, [c_void_p, POINTER(PoolDevice)]),
+        "mgv_diag_gather": (st, [c_void_p, POINTER(DiagGatherDesc), POINTER(c_double)]),
         "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
     }
     for name, (res, args) in sigs.items():
@@ -299,6 +319,17 @@ class Context:
         _call("mgv_diag_random_gather", self.h, table_bytes, n, ctas_per_sm, reps, byref(ms))
         return ms.value
 
+    def diag_gather(self, table_bytes: int, lookups: int, line_bytes: int = 32, method: int = 0,
+                    ctas_per_sm: int = 2, reps: int = 10, inflight: int = 4, lsu_warps: int = 8,
+                    tma_warps: int = 1, tma_share: float = 0.0) -> float:
+        """Milliseconds per pass of `lookups` random reads of line_bytes each
+        (method 0 LSU, 1 TMA gather4, 2 both; include/mgv_diag.h)."""
+        d = DiagGatherDesc(table_bytes, lookups, line_bytes, method, ctas_per_sm, reps, inflight, lsu_warps,
+                           tma_warps, tma_share)
+        ms = c_double()
+        _call("mgv_diag_gather", self.h, byref(d), byref(ms))
+        return ms.value
+
     # seeded columns ---------------------------------------------------
     def gen_uniform(self, dst, n, seed, stream_id, lo, rng, stream=None):
         _call("mgv_gen_uniform", self.h, c_void_p(_ptr(dst)), n, seed, stream_id, lo, rng, _stream(stream))
@@ -342,6 +373,13 @@ class Pool:
 
     def unregister_producer(self) -> None:
         _call("mgv_pool_unregister_producer", self.h)
+
+    def device_view(self) -> PoolDevice:
+        """mgv_pool_device_get: the view a kernel takes for device-side
+        acquire / release (include/mgv_device.cuh)."""
+        v = PoolDevice()
+        _call("mgv_pool_device_get", self.h, byref(v))
+        return v
 
     def stats(self) -> PoolStats:
         s = PoolStats()

@@ -113,8 +113,10 @@ def test_sum_modes(ctx, torch_cuda, tuned, mode):
         o.destroy()
 
 
-def test_config2_full_size(ctx, torch_cuda):
-    """Build 2^22 unique keys, probe 2^26 (the headline configuration)."""
+@pytest.mark.parametrize("lf", [0.4, 0.5])
+def test_config2_full_size(ctx, torch_cuda, lf):
+    """Build 2^22 unique keys, probe 2^26 (the headline configuration), at the
+    benchmark's load factor (0.4) and the context default (0.5)."""
     torch = torch_cuda
     nb, npb = 1 << 22, 1 << 26
     bk = torch.empty(nb, dtype=torch.int32, device="cuda")
@@ -125,8 +127,9 @@ def test_config2_full_size(ctx, torch_cuda):
     ctx.gen_uniform(bp, nb, 0x5EED0002, 1, 0, 1 << 20)
     hits = ctx.gen_probe_keys(pk, npb, 0x5EED0003, 0x5EED0002, nb, HIT, nb, (1 << 31) - nb)
     ctx.gen_uniform(pp, npb, 0x5EED0003, 2, 0, 1 << 20)
-    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb)
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, nb, lf)
     bhead.open(); bhead.consume_columns([bk, bp], nb); bhead.close()
+    assert hb.result().rows == nb
     probe.open(); probe.consume_columns([pk, pp], npb); probe.close()
     cnt, s = agg.result()
     hbk, hbp = bk.cpu().numpy(), bp.cpu().numpy()
@@ -163,6 +166,21 @@ def test_duplicates_and_load_factors(ctx, torch_cuda, lf):
     cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp, load_factor=lf)
     assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
     assert info.has_duplicates == 1
+
+
+@pytest.mark.parametrize("lf", [0.4, 0.5])
+def test_region_build_duplicates_large(ctx, torch_cuda, lf):
+    """2^18 build rows (the shared-memory region build, 2^16 rows and up)
+    with many duplicate keys: the region build's duplicate pass and every
+    duplicate's match, against the oracle."""
+    nb, npb = 1 << 18, 1 << 20
+    bk = po.gen_uniform(nb, 0x5EED0611, 0, 0, 1 << 17)  # about 2 copies per key
+    bp = po.gen_uniform(nb, 0x5EED0611, 1, -(1 << 31), 1 << 32)
+    pk = po.gen_uniform(npb, 0x5EED0611, 2, -1000, (1 << 17) + 2000)
+    pp = po.gen_uniform(npb, 0x5EED0611, 3, -(1 << 31), 1 << 32)
+    cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp, load_factor=lf)
+    assert (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+    assert info.has_duplicates == 1 and info.rows == nb
 
 
 def test_reserved_key_int32_min(ctx, torch_cuda):

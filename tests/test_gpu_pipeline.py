@@ -69,8 +69,10 @@ def test_partitioned_build_of_nothing(ctx, torch_cuda):
     assert got == [] and info.rows == 0
 
 
-def test_config3_full_size(ctx, torch_cuda):
-    """probe 2^27 rows, build 2^24 keys, 10% selectivity, Zipf(1) over 4096 groups."""
+@pytest.mark.parametrize("lf", [0.4, 0.5])
+def test_config3_full_size(ctx, torch_cuda, lf):
+    """probe 2^27 rows, build 2^24 keys, 10% selectivity, Zipf(1) over 4096
+    groups, at the benchmark's load factor (0.4) and the default (0.5)."""
     torch = torch_cuda
     nb, npb = 1 << 24, 1 << 27
     cols = [torch.empty(npb, dtype=torch.int32, device="cuda") for _ in range(4)]
@@ -81,8 +83,9 @@ def test_config3_full_size(ctx, torch_cuda):
     ctx.gen_uniform(cols[1], npb, seed, 2, 0, 1000)
     ctx.gen_zipf(cols[2], npb, seed, 3, 4096)
     ctx.gen_uniform(cols[3], npb, seed, 4, 0, 1 << 16)
-    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8)
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8, lf)
     part.open(); part.consume_columns([bk], nb); part.close()
+    assert hb.result().rows == nb
     sel.open(); sel.consume_columns(cols, npb); sel.close()
     got = gb.result()
     host = [c.cpu().numpy() for c in cols]

@@ -27,8 +27,8 @@ import statistics
 import sys
 import time
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-ROOT = os.path.dirname(HERE)
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "multigpu-vector_b200")
 HIT = 3865470566
 
 
@@ -462,7 +462,7 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
 
 
 def run(args) -> int:
-    sys.path.insert(0, HERE)
+    sys.path.insert(0, PKG)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))  # the CPU baselines time the oracle
     import torch
 
