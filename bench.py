@@ -10,9 +10,15 @@ producing COUNT(matches) and int64 SUM(build payload + probe payload).  The
 hash table is built once, outside the timed steps.
 
   value : probe tuples/s with the probe columns resident in HBM
-  e2e   : the same through the C ABI from pinned HOST memory: per step the
-          probe columns are written into pool buffers (H2D) and consumed
-          buffer by buffer, the result read back by close()
+  e2e   : the same through the C ABI from pinned HOST memory: per step
+          mgv_op_consume_host slices the host probe columns into pool
+          buffers, the copy of slice k+1 overlapping the probe of slice k,
+          and close() reads the result back
+
+The default run (N = 1) adds the other configurations' figures to the same
+line: select + aggregate, the select -> join -> group-by pipeline, the
+batched and served query mixes and the result delivery channel, each
+checked against the oracle or the plain path before it is printed.
 
 Multi-GPU: one process per GPU, each an independent replica of the
 workload (the probe shards with no exchange); value = all ranks' tuples /
@@ -127,16 +133,32 @@ class ClockSampler:
                 "samples": len(sm), "scope": scope}
 
 
-def cpu_probe_baseline(bk, bp, pk, pp, threads):
-    """Oracle chained-table probe (src/main8.cu:84-103 restated) on host cores."""
+def oracle_chain(bk, bp):
+    """The oracle's chained table (src/main8.cu:84-103 restated) on the build side."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     import pyoracle as po
 
-    chain = po.Chain(bk, bp)  # build once, not timed (the GPU table is built untimed too)
+    return po.Chain(bk, bp)
+
+
+def cpu_probe_baseline(chain, pk, pp, sample, threads):
+    """The oracle's chained-table probe on host cores, the table built once and
+    untimed (the GPU table is built untimed too): one core on a 2^22-row
+    sample (the reference's single-thread loop), all threads on `sample` rows."""
+    s1 = min(pk.size, 1 << 22)
     t0 = time.perf_counter()
-    res = chain.probe_agg_mt(pk, pp, threads)
-    dt = time.perf_counter() - t0
-    return pk.size / dt, dt, res
+    chain.probe_agg(pk[:s1], pp[:s1])
+    t1 = time.perf_counter() - t0
+    sa = min(pk.size, sample)
+    t0 = time.perf_counter()
+    chain.probe_agg_mt(pk[:sa], pp[:sa], threads)
+    ta = time.perf_counter() - t0
+    return {"value": s1 / t1, "unit": "tuples/s", "cores": 1, "kind": "port",
+            "sample": f"first {s1} probe rows against the full 2^22-key chained table (built once, untimed); "
+                      f"{t1:.2f} s on 1 core (the reference's single-thread probe loop, restated)",
+            "all_cores": {"value": sa / ta, "unit": "tuples/s", "cores": threads, "kind": "port",
+                          "sample": f"first {sa} probe rows, the same table; {ta:.2f} s on {threads} threads "
+                                    "(ours: the loop split over the host's threads)"}}
 
 
 def run_reference(args):
@@ -164,6 +186,10 @@ def run_reference(args):
             times.append(dt)
     ms = 1000.0 * statistics.median(times)
     v = sample / (ms / 1000.0)
+    s1 = min(sample, 1 << 22)  # the reference's own single-thread loop, for context
+    t0 = time.perf_counter()
+    chain.probe_agg(pk[:s1], pp[:s1])
+    one_core = s1 / (time.perf_counter() - t0)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "tuples/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -171,7 +197,9 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "build_rows": nb, "probe_rows": npb, "probe_rows_per_step_sample": sample},
         "cpu_baseline": {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
                          "sample": f"probe of {sample} rows per step against the full 2^22-key chained table "
-                                   f"(built once, untimed), {threads} threads"},
+                                   f"(built once, untimed), {threads} threads",
+                         "single_core": {"value": one_core, "unit": "tuples/s", "cores": 1,
+                                         "sample": f"first {s1} probe rows, 1 core"}},
         "e2e": {"value": v, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -318,22 +346,23 @@ def main():
     if not args.no_e2e:
         e2e = run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, (cnt, s))
 
-    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    # ---- oracle check of the timed run over every probe row, and the CPU baseline (rank 0, N = 1) ----
+    checked = None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = min(npb, args.cpu_sample)
         threads = os.cpu_count() or 1
-        v, dt, res = cpu_probe_baseline(bk.cpu().numpy(), bp.cpu().numpy(), pk[:sample].cpu().numpy(),
-                                        pp[:sample].cpu().numpy(), threads)
-        cpu = {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
-               "sample": f"first {sample} probe rows against the full 2^22-key chained table "
-                         f"(built once, untimed); {dt:.2f} s on {threads} threads"}
+        hbk, hbp, hpk, hpp = (t.cpu().numpy() for t in (bk, bp, pk, pp))
+        chain = oracle_chain(hbk, hbp)
+        want = chain.probe_agg_mt(hpk, hpp, threads)
+        assert want == (cnt, s), f"join result {(cnt, s)} differs from the oracle's {want}"
+        checked = f"oracle: COUNT and SUM equal the oracle's chained-table join over all {npb} probe rows"
+        cpu = cpu_probe_baseline(chain, hpk, hpp, args.cpu_sample, threads)
     # ---- the metric's other half: batched and served queries vs plain (N = 1) ----
     extras = {}
     if world == 1 and not args.no_extras:
         extras = run_extras(args, mgv, torch, ctx)
     return finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank,
-                  dist, (probe, agg, bhead, hb), nb, npb, tuning, extras)
+                  dist, (probe, agg, bhead, hb), nb, npb, tuning, extras, checked)
 
 
 def run_extras(args, mgv, torch, ctx):
@@ -348,13 +377,22 @@ def run_extras(args, mgv, torch, ctx):
     sub = argparse.Namespace(**vars(args))
     sub.steps, sub.warmup, sub.batch_config = 5, 3, None
     t0 = time.time()
+    sys.modules.setdefault("bench", sys.modules[__name__])
+    select = workloads.run_select(sub, mgv, torch, ctx, sys.modules[__name__], NoClock(), emit=False)
+    torch.cuda.empty_cache()
+    pipeline = workloads.run_pipeline(sub, mgv, torch, ctx, sys.modules[__name__], NoClock(), emit=False)
+    torch.cuda.empty_cache()
     batched = workloads.run_batched(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     served = workloads.run_served(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     torch.cuda.empty_cache()
     delivery = workloads.run_delivery(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     torch.cuda.empty_cache()
     at = {r["rate"]: r for r in served["rates"]}
+    keep = ("value", "unit", "ms", "workload", "roofline", "e2e", "cpu_baseline", "checked", "result", "gpu_launches",
+            "phases_ms")
     return {
+        "select": {k: select[k] for k in keep if k in select},
+        "pipeline": {k: pipeline[k] for k in keep if k in pipeline},
         "batched": {"value": batched["value"], "unit": "queries/s", "ms_per_batch": batched["ms"],
                     "plain_value": batched["plain"]["value"], "speedup_vs_plain": batched["speedup_vs_plain"],
                     "workload": batched["workload"], "batch_config": batched["batch_config"],
@@ -373,22 +411,18 @@ def run_extras(args, mgv, torch, ctx):
 
 
 def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, want):
+    """The same probe through the C ABI from pinned HOST columns: per step,
+    open -> mgv_op_consume_host (4 Mi-row slices through 3 pool buffers, the
+    copy of slice k+1 overlapping the probe of slice k) -> close."""
     cap = mgv.DEFAULT_BUFFER_ROWS
-    nbuf = (npb + cap - 1) // cap
-    pool = mgv.Pool(ctx, nbuf, cap, 2)
-    bufs = [pool.acquire() for _ in range(nbuf)]
+    pool = mgv.Pool(ctx, 3, cap, 2)
     hpk = pk.cpu().pin_memory()
     hpp = pp.cpu().pin_memory()
     e2e_steps = max(1, args.e2e_steps)
 
     def e2e_step():
         probe.open(stream)
-        for j, b in enumerate(bufs):
-            lo = j * cap
-            m = min(cap, npb - lo)
-            mgv.buffer_write(b, 0, hpk.data_ptr() + 4 * lo, m, stream)
-            mgv.buffer_write(b, 1, hpp.data_ptr() + 4 * lo, m, stream)
-            probe.consume(b, stream)
+        probe.consume_host(pool, [hpk.data_ptr(), hpp.data_ptr()], npb, stream)
         probe.close(stream)
 
     e2e_step()
@@ -407,15 +441,28 @@ def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world,
 
     e2e_s = replicas.max_over_ranks(dist, e0.elapsed_time(e1) / 1000.0, "cuda")
     e2e_value = replicas.job_rate(world, npb * e2e_steps, e2e_s)
-    for b in bufs:
-        pool.release(b)
+    # the host link's plain copy rate for the same bytes (pinned -> device), for context
+    h2d = 0.0
+    for _ in range(3):
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        with torch.cuda.stream(stream):
+            pk.copy_(hpk, non_blocking=True)
+            pp.copy_(hpp, non_blocking=True)
+        c1.record(stream)
+        stream.synchronize()
+        h2d = max(h2d, 8 * npb / (c0.elapsed_time(c1) / 1000.0) / 1e9)
     pool.destroy()
+    e2e_gbs = 8 * npb * e2e_steps / e2e_s / 1e9 / world
     return {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": 8 * npb, "d2h_bytes_per_step": 16,
-            "path": "mgv_buffer_write (pinned host -> pool buffer) + mgv_op_consume per 4Mi-row buffer"}
+            "h2d_gbs": e2e_gbs, "h2d_peak_gbs": h2d, "frac_of_h2d": e2e_gbs / h2d if h2d else None,
+            "path": "mgv_op_consume_host (pinned host columns -> 4 Mi-row slices through 3 pool buffers, "
+                    "copies overlapped with the probe) + mgv_op_close"}
 
 
 def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank, dist,
-           ops, nb, npb, tuning, extras=None):
+           ops, nb, npb, tuning, extras=None, checked=None):
     import replicas
 
     value = replicas.job_rate(world, npb * args.steps, elapsed)
@@ -444,6 +491,7 @@ def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, 
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "result": {"count": cnt, "sum": s},
+        "checked": checked or "count equals the generator's known hit count (oracle check skipped)",
     }
     line.update(extras or {})
     if rank == 0:

@@ -296,6 +296,20 @@ mgv_status mgv_op_consume(mgv_op *op, const mgv_buffer *buf, void *stream);
  * generator aliasing a user array into buffers, src/operators/generators.cu:55-90). */
 mgv_status mgv_op_consume_columns(mgv_op *op, const int32_t *const *cols, uint32_t ncols,
                                   uint64_t rows, void *stream);
+/* Host ingest: the reference's generator slicing a host column into pool
+ * buffers, and consumer::consume copying each buffer to the device before
+ * its consume kernel (src/operators/generators.cu:55-90,
+ * src/operators/exchange.cu:196-291), with the copies overlapped.  `rows`
+ * rows of the host columns host_cols[0..ncols) are cut into slices of the
+ * pool's buffer capacity (ncols <= the pool's columns; up to 3 buffers of
+ * `pool` in flight); slice k+1 is copied host -> device on the operator's
+ * own copy stream while slice k is consumed on `stream`, so the copies
+ * and the kernels run at the same time.  Pinned host memory copies fastest;
+ * pageable memory works.  Returns when every slice has been consumed: the
+ * host columns may be reused and the buffers are back in the pool.  Columns
+ * larger than device memory stream through a bounded pool this way. */
+mgv_status mgv_op_consume_host(mgv_op *op, mgv_pool *pool, const int32_t *const *host_cols, uint32_t ncols,
+                               uint64_t rows, void *stream);
 /* d_operator_t::close (src/operators/operator.cu:150-159): flushes, closes
  * the parents, waits for the stream and reports device errors. */
 mgv_status mgv_op_close(mgv_op *op, void *stream);

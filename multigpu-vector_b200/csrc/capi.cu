@@ -665,6 +665,14 @@ mgv_status mgv_op_destroy(mgv_op* o) {
         if (o->drain_done) cudaEventDestroy(o->drain_done);
         if (o->drain_stream) cudaStreamDestroy(o->drain_stream);
     }
+    if (o->in_stream) {
+        cudaStreamSynchronize(o->in_stream);
+        cudaStreamDestroy(o->in_stream);
+    }
+    for (cudaEvent_t ev : o->in_copied)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : o->in_consumed)
+        if (ev) cudaEventDestroy(ev);
     if (o->h_res) cudaFreeHost(o->h_res);
     if (o->rb_scratch) cudaFree(o->rb_scratch);
     if (o->gb_land) cudaFreeHost(o->gb_land);
@@ -1134,6 +1142,77 @@ mgv_status mgv_op_consume(mgv_op* o, const mgv_buffer* b, void* stream) {
     if (!o || !b) return fail(MGV_EINVAL, "NULL argument");
     if (b->rows > b->capacity) return fail(MGV_EINVAL, "buffer rows exceed capacity");
     return mgv_op_consume_columns(o, b->cols, b->ncols, b->rows, stream);
+}
+
+// Host ingest: slices of the host columns go through `depth` pool buffers;
+// the copy stream fills buffer k % depth once its previous slice has been
+// consumed, and the consume of slice k waits for its copy only.
+mgv_status mgv_op_consume_host(mgv_op* o, mgv_pool* pool, const int32_t* const* host_cols, uint32_t ncols,
+                               uint64_t rows, void* stream) {
+    constexpr uint32_t kDepth = 3;
+    if (!o || !pool || (!host_cols && ncols)) return fail(MGV_EINVAL, "NULL argument");
+    if (ncols == 0 || ncols > MGV_MAX_COLS || ncols > pool->ncols)
+        return fail(MGV_EINVAL, "column count must be 1..the pool's columns");
+    for (uint32_t c = 0; c < ncols; ++c)
+        if (!host_cols[c]) return fail(MGV_EINVAL, "host column is NULL");
+    if (pool->ctx->device != o->ctx->device) return fail(MGV_EINVAL, "pool and operator on different devices");
+    if (!all_open(o)) return fail(MGV_ESTATE, "chain is not open");
+    if (rows == 0) return MGV_OK;
+    MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+    cudaStream_t s = pick_stream(o->ctx, stream);
+    if (!o->in_stream) {
+        MGV_CUDA_TRY(cudaStreamCreateWithFlags(&o->in_stream, cudaStreamNonBlocking));
+        o->in_copied.assign(kDepth, nullptr);
+        o->in_consumed.assign(kDepth, nullptr);
+        for (uint32_t i = 0; i < kDepth; ++i) {
+            MGV_CUDA_TRY(cudaEventCreateWithFlags(&o->in_copied[i], cudaEventDisableTiming));
+            MGV_CUDA_TRY(cudaEventCreateWithFlags(&o->in_consumed[i], cudaEventDisableTiming));
+        }
+    }
+    const uint64_t cap = pool->capacity;
+    const uint64_t slices = (rows + cap - 1) / cap;
+    std::vector<mgv_buffer*> bufs;
+    for (uint32_t i = 0; i < kDepth && i < slices; ++i) {
+        mgv_buffer* b = nullptr;
+        const mgv_status st = mgv_buffer_acquire(pool, bufs.empty() ? 1000000u : 0u, &b);
+        if (st != MGV_OK) {
+            if (bufs.empty()) return st;
+            break;  // fewer buffers in flight
+        }
+        bufs.push_back(b);
+    }
+    const uint32_t depth = (uint32_t)bufs.size();
+    mgv_status st = MGV_OK;
+    // the copy stream starts after what `s` already holds (earlier consumes
+    // may still read buffers that this call reuses)
+    cudaError_t e = cudaEventRecord(o->in_consumed[0], s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(o->in_stream, o->in_consumed[0], 0);
+    uint64_t k = 0;
+    for (; k < slices && e == cudaSuccess && st == MGV_OK; ++k) {
+        const uint32_t j = (uint32_t)(k % depth);
+        mgv_buffer* b = bufs[j];
+        const uint64_t lo = k * cap;
+        const uint32_t m = (uint32_t)std::min<uint64_t>(cap, rows - lo);
+        if (k >= depth) e = cudaStreamWaitEvent(o->in_stream, o->in_consumed[j], 0);
+        for (uint32_t c = 0; c < ncols && e == cudaSuccess; ++c)
+            e = cudaMemcpyAsync(b->cols[c], host_cols[c] + lo, sizeof(int32_t) * m, cudaMemcpyHostToDevice,
+                                o->in_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(o->in_copied[j], o->in_stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, o->in_copied[j], 0);
+        if (e != cudaSuccess) break;
+        b->rows = m;
+        st = consume_cols(o, b->cols, ncols, m, s);
+        if (st == MGV_OK) e = cudaEventRecord(o->in_consumed[j], s);
+    }
+    // every slice consumed (or the failure reached) before the buffers go back
+    const cudaError_t w = cudaStreamSynchronize(s);
+    const cudaError_t w2 = cudaStreamSynchronize(o->in_stream);
+    for (mgv_buffer* b : bufs) mgv_buffer_release(pool, b);
+    if (st != MGV_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "mgv_op_consume_host");
+    if (w != cudaSuccess) return cuda_fail(w, "mgv_op_consume_host: stream");
+    if (w2 != cudaSuccess) return cuda_fail(w2, "mgv_op_consume_host: copy stream");
+    return MGV_OK;
 }
 
 }  // extern "C"

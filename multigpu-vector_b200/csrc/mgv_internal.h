@@ -174,6 +174,10 @@ struct Op {
     std::vector<uint64_t> pt_hist;        // rows per partition (read back at close)
     bool hb_fresh = false;  // opened, nothing consumed yet: the table is not cleared yet
     bool hb_partitioned = false;  // the rows being consumed are a partition op's run on the table's radix bits
+    // host ingest (mgv_op_consume_host): the copy stream and, per buffer in
+    // flight, events for "slice copied" and "slice consumed"
+    cudaStream_t in_stream = nullptr;
+    std::vector<cudaEvent_t> in_copied, in_consumed;
     // shared-memory build scratch (hash_build), grown on demand
     void* rb_scratch = nullptr;
     size_t rb_bytes = 0;

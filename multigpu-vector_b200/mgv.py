@@ -235,6 +235,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                        c_void_p, c_void_p]),
         "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
         "mgv_pool_device_get": (st, [c_void_p, POINTER(PoolDevice)]),
+        "mgv_op_consume_host": (st, [c_void_p, c_void_p, POINTER(c_void_p), c_uint32, c_uint64, c_void_p]),
         "mgv_diag_gather": (st, [c_void_p, POINTER(DiagGatherDesc), POINTER(c_double)]),
         "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
     }
@@ -468,6 +469,21 @@ class Op:
     def consume_columns(self, cols, rows: int, stream=None) -> None:
         arr = (c_void_p * max(1, len(cols)))(*[_ptr(c) for c in cols])
         _call("mgv_op_consume_columns", self.h, arr, len(cols), rows, _stream(stream))
+
+    def consume_host(self, pool: "Pool", host_cols, rows: int, stream=None) -> None:
+        """mgv_op_consume_host: rows of host columns (numpy arrays, pinned
+        torch tensors or raw host addresses) pushed through the chain in
+        slices of the pool's buffers, copies overlapped with the consumes."""
+        ptrs = []
+        for c in host_cols:
+            if isinstance(c, int):
+                ptrs.append(c)
+            elif hasattr(c, "ctypes"):
+                ptrs.append(c.ctypes.data)
+            else:
+                ptrs.append(c.data_ptr())
+        arr = (c_void_p * max(1, len(ptrs)))(*ptrs)
+        _call("mgv_op_consume_host", self.h, pool.h, arr, len(ptrs), rows, _stream(stream))
 
     def close(self, stream=None) -> None:
         _call("mgv_op_close", self.h, _stream(stream))

@@ -100,6 +100,44 @@ void or_select_agg(const int32_t *f, const int32_t *v, size_t n, int32_t bound,
     *sum = s;
 }
 
+typedef struct select_job {
+    const int32_t *f, *v;
+    uint64_t lo, hi;
+    int32_t bound;
+    int64_t count, sum;
+} select_job;
+
+static void *select_worker(void *arg) {
+    select_job *j = (select_job *)arg;
+    or_select_agg(j->f + j->lo, j->v ? j->v + j->lo : NULL, j->hi - j->lo, j->bound, &j->count, &j->sum);
+    return NULL;
+}
+
+/* The same split over `threads` host threads. */
+void or_select_agg_mt(const int32_t *f, const int32_t *v, size_t n, int32_t bound, int threads,
+                      int64_t *count, int64_t *sum) {
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t tid[256];
+    select_job jobs[256];
+    for (int i = 0; i < threads; ++i) {
+        jobs[i].f = f;
+        jobs[i].v = v;
+        jobs[i].bound = bound;
+        jobs[i].lo = n * (uint64_t)i / (uint64_t)threads;
+        jobs[i].hi = n * (uint64_t)(i + 1) / (uint64_t)threads;
+        pthread_create(&tid[i], NULL, select_worker, &jobs[i]);
+    }
+    int64_t c = 0, s = 0;
+    for (int i = 0; i < threads; ++i) {
+        pthread_join(tid[i], NULL);
+        c += jobs[i].count;
+        s += jobs[i].sum;
+    }
+    *count = c;
+    *sum = s;
+}
+
 /* ---------------------------------------------------------------------- */
 /* chained hash join (src/main8.cu:84-103)                                */
 /* ---------------------------------------------------------------------- */
@@ -345,20 +383,58 @@ uint64_t or_groupby(const int32_t *groups, const int32_t *values, const int32_t 
  * key contributes one output tuple; the tuples are grouped by the probe's
  * group column into int64 SUM(value) and COUNT.  The radix partition that
  * precedes the build on the GPU does not change this result. */
-uint64_t or_run_query(const or_query *q, or_group_row *out, uint64_t cap,
-                      int64_t *total_count, int64_t *total_sum) {
-    or_chain_table t;
-    or_chain_build(&t, q->build_keys, NULL, q->build_rows, 0, 0);
-    int32_t *mult = (int32_t *)malloc(sizeof(int32_t) * (q->probe_rows ? q->probe_rows : 1));
+typedef struct query_job {
+    const or_query *q;
+    const or_chain_table *t;
+    int32_t *mult;
+    uint64_t lo, hi;
+    int64_t count, sum;
+} query_job;
+
+/* The select + probe of rows [lo, hi): each row's match multiplicity. */
+static void *query_probe(void *arg) {
+    query_job *j = (query_job *)arg;
+    const or_query *q = j->q;
     int64_t tc = 0, ts = 0;
-    for (uint64_t i = 0; i < q->probe_rows; ++i) {
-        mult[i] = 0;
+    for (uint64_t i = j->lo; i < j->hi; ++i) {
+        j->mult[i] = 0;
         if (q->probe_filter[i] <= q->filter_bound) {
-            uint64_t mu = or_chain_matches(&t, q->probe_key[i]);
-            mult[i] = (int32_t)mu;
+            uint64_t mu = or_chain_matches(j->t, q->probe_key[i]);
+            j->mult[i] = (int32_t)mu;
             tc += (int64_t)mu;
             ts += (int64_t)mu * q->probe_value[i];
         }
+    }
+    j->count = tc;
+    j->sum = ts;
+    return NULL;
+}
+
+/* The query with its select + probe phase split over `threads` host
+ * threads (the table is read-only); build and group-by stay on one. */
+uint64_t or_run_query_mt(const or_query *q, or_group_row *out, uint64_t cap,
+                         int64_t *total_count, int64_t *total_sum, int threads) {
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    or_chain_table t;
+    or_chain_build(&t, q->build_keys, NULL, q->build_rows, 0, 0);
+    int32_t *mult = (int32_t *)malloc(sizeof(int32_t) * (q->probe_rows ? q->probe_rows : 1));
+    pthread_t tid[256];
+    query_job jobs[256];
+    for (int i = 0; i < threads; ++i) {
+        jobs[i].q = q;
+        jobs[i].t = &t;
+        jobs[i].mult = mult;
+        jobs[i].lo = q->probe_rows * (uint64_t)i / (uint64_t)threads;
+        jobs[i].hi = q->probe_rows * (uint64_t)(i + 1) / (uint64_t)threads;
+        if (threads == 1) query_probe(&jobs[i]);
+        else pthread_create(&tid[i], NULL, query_probe, &jobs[i]);
+    }
+    int64_t tc = 0, ts = 0;
+    for (int i = 0; i < threads; ++i) {
+        if (threads > 1) pthread_join(tid[i], NULL);
+        tc += jobs[i].count;
+        ts += jobs[i].sum;
     }
     uint64_t g = or_groupby(q->probe_group, q->probe_value, mult, q->probe_rows, out, cap);
     free(mult);
@@ -366,4 +442,9 @@ uint64_t or_run_query(const or_query *q, or_group_row *out, uint64_t cap,
     if (total_count) *total_count = tc;
     if (total_sum) *total_sum = ts;
     return g;
+}
+
+uint64_t or_run_query(const or_query *q, or_group_row *out, uint64_t cap,
+                      int64_t *total_count, int64_t *total_sum) {
+    return or_run_query_mt(q, out, cap, total_count, total_sum, 1);
 }

@@ -41,6 +41,8 @@ uint32_t or_hash_murmur(uint32_t x);
 size_t or_select_rows(const int32_t *a, size_t n, int32_t bound, int32_t *out);
 void or_select_agg(const int32_t *f, const int32_t *v, size_t n, int32_t bound,
                    int64_t *count, int64_t *sum);
+void or_select_agg_mt(const int32_t *f, const int32_t *v, size_t n, int32_t bound, int threads,
+                      int64_t *count, int64_t *sum);
 
 /* ---- chained hash join ------------------------------------------------ */
 typedef struct or_chain_table {
@@ -92,6 +94,9 @@ typedef struct or_query {
 
 uint64_t or_run_query(const or_query *q, or_group_row *out, uint64_t cap,
                       int64_t *total_count, int64_t *total_sum);
+/* The same with the select + probe phase on `threads` host threads. */
+uint64_t or_run_query_mt(const or_query *q, or_group_row *out, uint64_t cap,
+                         int64_t *total_count, int64_t *total_sum, int threads);
 
 #ifdef __cplusplus
 }

@@ -61,6 +61,7 @@ def lib() -> ctypes.CDLL:
             "or_hash_murmur": (c_uint32, [c_uint32]),
             "or_select_rows": (c_size_t, [P, c_size_t, c_int32, P]),
             "or_select_agg": (None, [P, P, c_size_t, c_int32, POINTER(c_int64), POINTER(c_int64)]),
+            "or_select_agg_mt": (None, [P, P, c_size_t, c_int32, c_int, POINTER(c_int64), POINTER(c_int64)]),
             "or_chain_build": (c_int, [POINTER(ChainTable), P, P, c_uint64, c_int, c_int32]),
             "or_chain_free": (None, [POINTER(ChainTable)]),
             "or_chain_probe_agg": (None, [POINTER(ChainTable), P, P, c_uint64, c_int, c_int,
@@ -72,6 +73,7 @@ def lib() -> ctypes.CDLL:
             "or_partition": (None, [P, c_uint64, c_uint32, c_uint32, P, P, P, P]),
             "or_groupby": (c_uint64, [P, P, P, c_uint64, P, c_uint64]),
             "or_run_query": (c_uint64, [POINTER(Query), P, c_uint64, POINTER(c_int64), POINTER(c_int64)]),
+            "or_run_query_mt": (c_uint64, [POINTER(Query), P, c_uint64, POINTER(c_int64), POINTER(c_int64), c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -164,6 +166,16 @@ def select_agg(f: np.ndarray, v: np.ndarray | None, bound: int):
     return c.value, s.value
 
 
+def select_agg_mt(f: np.ndarray, v: np.ndarray | None, bound: int, threads: int):
+    """select_agg split over `threads` host threads."""
+    f = np.ascontiguousarray(f, np.int32)
+    v = None if v is None else np.ascontiguousarray(v, np.int32)
+    c, s = c_int64(), c_int64()
+    lib().or_select_agg_mt(_p(f), None if v is None else _p(v), f.size, bound, threads, ctypes.byref(c),
+                           ctypes.byref(s))
+    return c.value, s.value
+
+
 class Chain:
     """The reference's chained table (src/main8.cu:84-103), with payloads."""
 
@@ -238,12 +250,16 @@ def groupby(groups, values, mult=None) -> np.ndarray:
     return out[:n]
 
 
-def run_query(build_keys, probe_key, probe_filter, probe_group, probe_value, bound):
-    """select(filter <= bound) -> join(build keys) -> group-by(group): SUM(value), COUNT."""
+def run_query(build_keys, probe_key, probe_filter, probe_group, probe_value, bound, threads=1):
+    """select(filter <= bound) -> join(build keys) -> group-by(group): SUM(value), COUNT
+    (the select + probe phase on `threads` host threads)."""
     arrs = [np.ascontiguousarray(a, np.int32) for a in (build_keys, probe_key, probe_filter, probe_group, probe_value)]
     q = Query(_p(arrs[0]), arrs[0].size, _p(arrs[1]), _p(arrs[2]), _p(arrs[3]), _p(arrs[4]), arrs[1].size, bound)
     tc, ts = c_int64(), c_int64()
-    n = lib().or_run_query(ctypes.byref(q), None, 0, ctypes.byref(tc), ctypes.byref(ts))
-    out = np.zeros(max(1, n), GROUP_DTYPE)
-    lib().or_run_query(ctypes.byref(q), _p(out), n, ctypes.byref(tc), ctypes.byref(ts))
+    cap = 1 << 17  # more groups than any workload here has; rerun with the exact count otherwise
+    out = np.zeros(cap, GROUP_DTYPE)
+    n = lib().or_run_query_mt(ctypes.byref(q), _p(out), cap, ctypes.byref(tc), ctypes.byref(ts), threads)
+    if n > cap:
+        out = np.zeros(n, GROUP_DTYPE)
+        lib().or_run_query_mt(ctypes.byref(q), _p(out), n, ctypes.byref(tc), ctypes.byref(ts), threads)
     return out[:n], tc.value, ts.value

@@ -46,8 +46,45 @@ def _line(args, metric, value, unit, ms, workload, extra, clk, higher=True):
         print(json.dumps(d), flush=True)
 
 
-def run_select(args, mgv, torch, ctx, bench, clk):
+def _h2d_gbs(torch, host, dev, stream, reps=3):
+    """Plain pinned host -> device copy rate of `host` (GB/s, best of reps)."""
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            dev.copy_(host, non_blocking=True)
+        e1.record(stream)
+        stream.synchronize()
+        best = max(best, host.numel() * host.element_size() / (e0.elapsed_time(e1) / 1000.0) / 1e9)
+    return best
+
+
+def _cpu_pair(one_fn, one_rows, all_fn, all_rows, total_rows, unit, what_one, what_all):
+    """1-core reference-style loop and all-core port, each timed on a sample and
+    scaled to the workload's rows; returns the cpu_baseline object (1 core)
+    with the all-core figure beside it, labelled."""
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    one_fn()
+    t1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    all_fn(threads)
+    ta = time.perf_counter() - t0
+    return {"value": one_rows / t1, "unit": unit, "cores": 1, "kind": "port",
+            "sample": f"{what_one}: {one_rows} rows in {t1:.3f} s on 1 core (the reference's own single-thread "
+                      f"CPU loop, restated)",
+            "all_cores": {"value": all_rows / ta, "unit": unit, "cores": threads, "kind": "port",
+                          "sample": f"{what_all}: {all_rows} rows in {ta:.3f} s on {threads} threads (ours: "
+                                    "the same loop split over the host's threads)"}}
+
+
+def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
+    """Select + aggregate (c0 <= 2^30 - 1 -> COUNT, SUM(c1)) over 2^22 rows."""
+    import pyoracle as po
+
     n = 1 << 22
+    bound = (1 << 30) - 1
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         c0 = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -57,8 +94,9 @@ def run_select(args, mgv, torch, ctx, bench, clk):
         flush = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
     ctx.gen_uniform(c0, n, 0x5EED0001, 0, 0, 1 << 31, stream=stream)
     ctx.gen_uniform(c1, n, 0x5EED0001, 1, 0, 1 << 20, stream=stream)
-    head, agg = mgv.create_sum_select_pipeline(ctx, (1 << 30) - 1, 0, 1)
+    head, agg = mgv.create_sum_select_pipeline(ctx, bound, 0, 1)
     times, ktimes = [], []
+    launches0 = ctx.launches
     h0 = time.time()
     for i in range(args.warmup + args.steps):
         with torch.cuda.stream(stream):
@@ -77,36 +115,65 @@ def run_select(args, mgv, torch, ctx, bench, clk):
             times.append(e0.elapsed_time(e1) / 1000.0)
             ktimes.append(k0.elapsed_time(k1) / 1000.0)
     clk.mark(h0, time.time())
+    launches = (ctx.launches - launches0) * args.steps // (args.warmup + args.steps)
     cnt, s = agg.result()
+    del flush
     t = statistics.median(times)
     kt = statistics.median(ktimes)
     peak, kind = bench.measured_peaks()
-    # CPU baseline: the oracle's restatement of sum_select_cpu (src/main9.cu:56-61), one core, all rows
-    import pyoracle as po
-
     hc0, hc1 = c0.cpu().numpy(), c1.cpu().numpy()
-    ct = time.perf_counter()
-    for _ in range(5):
-        ref = po.select_agg(hc0, hc1, (1 << 30) - 1)
-    cdt = (time.perf_counter() - ct) / 5
-    assert ref == (cnt, s), (ref, cnt, s)
-    cpu = {"value": n / cdt, "unit": "rows/s", "cores": 1, "kind": "port",
-           "sample": f"all 2^22 rows, mean of 5 runs ({cdt * 1e3:.1f} ms each)"}
-    _line(args, "select+aggregate rows/s", n / t, "rows/s", 1000 * t,
-          "select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between steps",
-          {"roofline": {"bound": "hbm", "achieved": 8 * n / kt / 1e9, "peak": peak, "unit": "GB/s",
-                        "frac": 8 * n / kt / 1e9 / peak, "peak_kind": kind, "kernel_ms": 1000 * kt,
-                        "algorithmic_bytes_per_launch": 8 * n},
-           "step_gbs": 8 * n / t / 1e9,
-           "result": {"count": cnt, "sum": s}, "cpu_baseline": cpu,
-           "note": "step = open -> consume -> close incl. the host read-back; 33.5 MB per step; the roofline is "
-                   "the consume's kernel (k_select_agg), timed with events around it"}, clk)
+    assert po.select_agg_mt(hc0, hc1, bound, os.cpu_count() or 1) == (cnt, s), "select result differs from the oracle"
+    cpu = _cpu_pair(lambda: po.select_agg(hc0, hc1, bound), n, lambda th: po.select_agg_mt(hc0, hc1, bound, th), n,
+                    n, "rows/s", "sum_select_cpu-style loop over all 2^22 rows", "the same over all 2^22 rows")
+    # end to end: pinned host columns through mgv_op_consume_host (4 slices of 1 Mi rows)
+    h0c, h1c = c0.cpu().pin_memory(), c1.cpu().pin_memory()
+    pool = mgv.Pool(ctx, 3, 1 << 20, 2)
+    et = []
+    for i in range(3 + max(3, args.steps // 4)):
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        head.open(stream)
+        head.consume_host(pool, [h0c.data_ptr(), h1c.data_ptr()], n, stream)
+        head.close(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= 3:
+            et.append(e0.elapsed_time(e1) / 1000.0)
+    assert agg.result() == (cnt, s)
+    e2e_t = statistics.median(et)
+    with torch.cuda.stream(stream):
+        both = torch.empty(2 * n, dtype=torch.int32, device="cuda")
+    hb = torch.cat([h0c, h1c]).pin_memory()
+    h2d = _h2d_gbs(torch, hb, both, stream)
+    pool.destroy()
+    workload = "select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between steps"
+    extra = {"roofline": {"bound": "hbm", "achieved": 8 * n / kt / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": 8 * n / kt / 1e9 / peak, "peak_kind": kind, "kernel_ms": 1000 * kt,
+                          "algorithmic_bytes_per_launch": 8 * n, "kernel": "k_select_agg"},
+             "step_gbs": 8 * n / t / 1e9,
+             "e2e": {"value": n / e2e_t, "unit": "rows/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 16,
+                     "ms_per_step": 1000 * e2e_t, "h2d_gbs": 8 * n / e2e_t / 1e9, "h2d_peak_gbs": h2d,
+                     "frac_of_h2d": 8 * n / e2e_t / 1e9 / h2d,
+                     "path": "mgv_op_consume_host (pinned host columns, 1 Mi-row slices through 3 pool buffers, "
+                             "copies overlapped with the consumes) + close"},
+             "result": {"count": cnt, "sum": s}, "cpu_baseline": cpu, "gpu_launches": launches,
+             "checked": "oracle: COUNT and SUM equal the oracle's select + aggregate over all 2^22 rows",
+             "note": "step = open -> consume -> close incl. the host read-back; 33.5 MB per step; the roofline is "
+                     "the consume's kernel (k_select_agg), timed with events around it"}
+    if emit:
+        _line(args, "select+aggregate rows/s", n / t, "rows/s", 1000 * t, workload, extra, clk)
     head.destroy()
     agg.destroy()
+    return {"value": n / t, "unit": "rows/s", "ms": 1000 * t, "workload": workload, **extra}
 
 
-def run_pipeline(args, mgv, torch, ctx, bench, clk):
+def run_pipeline(args, mgv, torch, ctx, bench, clk, emit=True):
+    """select -> join -> group-by over 2^27 probe rows with a 2^24-key radix-partitioned build."""
+    import numpy as np
+    import pyoracle as po
+
     nb, npb = 1 << 24, 1 << 27
+    lf = args.pipeline_load_factor
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         bk = torch.empty(nb, dtype=torch.int32, device="cuda")
@@ -117,9 +184,9 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
     ctx.gen_uniform(cols[1], npb, seed, 2, 0, 1000, stream=stream)
     ctx.gen_zipf(cols[2], npb, seed, 3, 4096, stream=stream)
     ctx.gen_uniform(cols[3], npb, seed, 4, 0, 1 << 16, stream=stream)
-    qualifying = int((cols[1] <= 99).sum().item())
-    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8, args.pipeline_load_factor)
+    part, hb, sel, gb = mgv.create_join_groupby_pipeline(ctx, nb, 4096, 99, 8, lf)
     bt, pt = [], []
+    launches0 = ctx.launches
     h0 = time.time()
     for i in range(args.warmup + args.steps):
         e0, e1, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), \
@@ -134,40 +201,79 @@ def run_pipeline(args, mgv, torch, ctx, bench, clk):
             bt.append(e0.elapsed_time(e1) / 1000.0)
             pt.append(e1.elapsed_time(e2) / 1000.0)
     clk.mark(h0, time.time())
+    launches = (ctx.launches - launches0) * args.steps // (args.warmup + args.steps)
     res = gb.result()
-    total = sum(c for _, _, c in res)
-    assert total == qualifying, (total, qualifying)  # every probe key is a build key
     b, p_ = statistics.median(bt), statistics.median(pt)
     peak, kind = bench.measured_peaks()
     alg = 16 * npb + 4 * nb
-    # CPU baseline: the oracle's select -> chained-table join -> group-by on one core; the full
-    # 2^24-key build is timed once, the probe side on a 2^22-row sample, scaled to 2^27 rows
-    import pyoracle as po
-
-    sample = 1 << 22
+    # the oracle over every row (select + probe on all host threads)
+    threads = os.cpu_count() or 1
     hb_keys = bk.cpu().numpy()
-    hcols = [c[:sample].cpu().numpy() for c in cols]
+    hcols = [c.cpu().numpy() for c in cols]
+    want, _, _ = po.run_query(hb_keys, *hcols, 99, threads=threads)
+    assert res == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want], "pipeline differs from the oracle"
+    total = sum(c for _, _, c in res)
+    # CPU baselines: the full 2^24-key chained-table build timed once, the probe side on a sample, scaled
     ct = time.perf_counter()
     po.run_query(hb_keys, hcols[0][:0], hcols[1][:0], hcols[2][:0], hcols[3][:0], 99)
     t_build = time.perf_counter() - ct
+    s1, sa = 1 << 22, 1 << 24
     ct = time.perf_counter()
-    po.run_query(hb_keys, *hcols, 99)
-    t_probe = time.perf_counter() - ct - t_build
-    cpu_s = t_build + t_probe * npb / sample
-    cpu = {"value": npb / cpu_s, "unit": "rows/s", "cores": 1, "kind": "port",
-           "sample": f"full 2^24-key chained-table build ({t_build:.2f} s) + select/probe/group-by of the "
-                     f"first 2^22 probe rows ({t_probe:.2f} s), scaled to 2^27 rows"}
-    _line(args, "select->join->group-by probe rows/s", npb / (b + p_), "rows/s", 1000 * (b + p_),
-          "select (filter <= 99 of U[0,1000)) -> join (2^27 probe rows, key over 2^24 build keys) -> group-by "
-          "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key bits, "
-          f"table load factor {args.pipeline_load_factor}",
-          {"roofline": {"bound": "hbm", "achieved": alg / (b + p_) / 1e9, "peak": peak, "unit": "GB/s",
-                        "frac": alg / (b + p_) / 1e9 / peak, "peak_kind": kind,
-                        "algorithmic_bytes_per_step": alg},
-           "phases_ms": {"partition+build": 1000 * b, "select+probe+groupby": 1000 * p_},
-           "result": {"groups": len(res), "count": total}, "cpu_baseline": cpu}, clk)
+    po.run_query(hb_keys, *[c[:s1] for c in hcols], 99)
+    t1 = time.perf_counter() - ct - t_build
+    ct = time.perf_counter()
+    po.run_query(hb_keys, *[c[:sa] for c in hcols], 99, threads=threads)
+    ta = time.perf_counter() - ct - t_build
+    cpu1 = t_build + t1 * npb / s1
+    cpua = t_build + ta * npb / sa
+    cpu = {"value": npb / cpu1, "unit": "rows/s", "cores": 1, "kind": "port",
+           "sample": f"full 2^24-key chained-table build ({t_build:.2f} s) + select/probe/group-by of the first "
+                     f"2^22 probe rows ({t1:.2f} s) on 1 core, scaled to 2^27 rows",
+           "all_cores": {"value": npb / cpua, "unit": "rows/s", "cores": threads, "kind": "port",
+                         "sample": f"the same build (1 core) + the first 2^24 probe rows with the select/probe "
+                                   f"split over {threads} threads ({ta:.2f} s), scaled to 2^27 rows (ours)"}}
+    # end to end: pinned host build keys and probe columns through mgv_op_consume_host
+    hbk = bk.cpu().pin_memory()
+    hpc = [c.cpu().pin_memory() for c in cols]
+    pool1 = mgv.Pool(ctx, 3, mgv.DEFAULT_BUFFER_ROWS, 1)
+    pool4 = mgv.Pool(ctx, 3, mgv.DEFAULT_BUFFER_ROWS, 4)
+    et = []
+    for i in range(1 + max(2, args.steps // 10)):
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        part.open(stream); part.consume_host(pool1, [hbk.data_ptr()], nb, stream); part.close(stream)
+        sel.open(stream); sel.consume_host(pool4, [c.data_ptr() for c in hpc], npb, stream); sel.close(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= 1:
+            et.append(e0.elapsed_time(e1) / 1000.0)
+    assert gb.result() == res
+    e2e_t = statistics.median(et)
+    h2d = _h2d_gbs(torch, hpc[0], cols[0], stream)
+    pool1.destroy(); pool4.destroy()
+    del hpc, hbk
+    workload = ("select (filter <= 99 of U[0,1000)) -> join (2^27 probe rows, key over 2^24 build keys) -> group-by "
+                "(Zipf(1) over 4096 groups, int64 SUM(value U[0,2^16)) + COUNT); build radix-partitioned on 8 key "
+                f"bits, table load factor {lf}")
+    extra = {"roofline": {"bound": "hbm", "achieved": alg / (b + p_) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": alg / (b + p_) / 1e9 / peak, "peak_kind": kind,
+                          "algorithmic_bytes_per_step": alg, "scope": "whole step (partition + build + probe)"},
+             "phases_ms": {"partition+build": 1000 * b, "select+probe+groupby": 1000 * p_},
+             "e2e": {"value": npb / e2e_t, "unit": "rows/s", "h2d_bytes_per_step": alg,
+                     "d2h_bytes_per_step": 24 * len(res), "ms_per_step": 1000 * e2e_t, "h2d_gbs": alg / e2e_t / 1e9,
+                     "h2d_peak_gbs": h2d, "frac_of_h2d": alg / e2e_t / 1e9 / h2d,
+                     "path": "mgv_op_consume_host of the pinned build keys (partition -> build) and of the four "
+                             "pinned probe columns (select -> probe -> group-by), 4 Mi-row slices through 3 pool "
+                             "buffers, copies overlapped with the consumes"},
+             "result": {"groups": len(res), "count": total}, "cpu_baseline": cpu, "gpu_launches": launches,
+             "checked": "oracle: every group's SUM and COUNT equal the oracle's select -> chained-table join -> "
+                        "group-by over all 2^27 probe rows"}
+    if emit:
+        _line(args, "select->join->group-by probe rows/s", npb / (b + p_), "rows/s", 1000 * (b + p_), workload,
+              extra, clk)
     for o in (sel, gb, hb, part):
         o.destroy()
+    return {"value": npb / (b + p_), "unit": "rows/s", "ms": 1000 * (b + p_), "workload": workload, **extra}
 
 
 def run_delivery(args, mgv, torch, ctx, bench, clk, emit=True):
