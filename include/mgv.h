@@ -272,6 +272,19 @@ typedef struct mgv_partition_desc {
     uint64_t max_rows;
 } mgv_partition_desc;
 
+/* The routing step of split / hash_exchange on its own
+ * (src/operators/split.cu:49-118, src/main9.cu:104-148), for callers that
+ * move the partitions themselves (the multi-GPU hash exchange sends
+ * partition p to rank p): the rows of device columns cols[0..ncols) are
+ * written partition-major, by (cols[key_col] >> radix_shift) &
+ * (2^radix_bits - 1), into `out` (column c at out + c * out_stride,
+ * out_stride >= rows), and counts[p] (host memory, 2^radix_bits entries)
+ * receives the rows of partition p.  Rows keep no order within a partition.
+ * radix_bits in 1..12.  Waits for `stream`. */
+mgv_status mgv_partition_columns(mgv_ctx *ctx, const int32_t *const *cols, uint32_t ncols, uint64_t rows,
+                                 uint32_t key_col, uint32_t radix_bits, uint32_t radix_shift, int32_t *out,
+                                 uint64_t out_stride, uint64_t *counts, void *stream);
+
 mgv_status mgv_op_create_select(mgv_ctx *ctx, const mgv_select_desc *desc, mgv_op *parent,
                                 mgv_op **out);
 mgv_status mgv_op_create_groupby(mgv_ctx *ctx, const mgv_groupby_desc *desc, mgv_op **out);
@@ -448,9 +461,11 @@ typedef struct mgv_server_config {
     uint32_t max_inflight;   /* batches on the GPU at once (0 = 2, max 16)    */
     float load_factor;       /* resident join tables (0 = context default)    */
     uint32_t plain;          /* 1 = one request at a time, operator API       */
-    uint32_t batch_solo;     /* 0: a request that arrives to an idle server
-                              * runs alone through the operator chain (lower
-                              * latency); 1: it is batched like any other     */
+    uint32_t batch_solo;     /* 0: while nothing is in flight and at most two
+                              * requests wait, the oldest runs alone through
+                              * the operator chain (lower latency); batches
+                              * form once a longer queue builds up;
+                              * 1: every request is batched                   */
     uint32_t reserved;
 } mgv_server_config;
 

@@ -1144,6 +1144,41 @@ mgv_status mgv_op_consume(mgv_op* o, const mgv_buffer* b, void* stream) {
     return mgv_op_consume_columns(o, b->cols, b->ncols, b->rows, stream);
 }
 
+mgv_status mgv_partition_columns(mgv_ctx* ctx, const int32_t* const* cols, uint32_t ncols, uint64_t rows,
+                                 uint32_t key_col, uint32_t radix_bits, uint32_t radix_shift, int32_t* out,
+                                 uint64_t out_stride, uint64_t* counts, void* stream) {
+    if (!ctx || !counts || (!cols && ncols) || (rows && !out)) return fail(MGV_EINVAL, "NULL argument");
+    if (ncols == 0 || ncols > MGV_MAX_COLS || key_col >= ncols) return fail(MGV_EINVAL, "column out of range");
+    if (radix_bits < 1 || radix_bits > 12 || radix_shift > 31) return fail(MGV_EINVAL, "radix bits out of range");
+    if (out_stride < rows) return fail(MGV_EINVAL, "out_stride is smaller than rows");
+    for (uint32_t c = 0; c < ncols; ++c)
+        if (rows && !cols[c]) return fail(MGV_EINVAL, "column is NULL");
+    const uint32_t P = 1u << radix_bits;
+    std::memset(counts, 0, sizeof(uint64_t) * P);
+    if (rows == 0) return MGV_OK;
+    MGV_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t s = pick_stream(ctx, stream);
+    // scratch: [histogram -> cursors (P) | rows stored, rows per partition (1 + P)]
+    unsigned long long* d = nullptr;
+    MGV_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(unsigned long long) * (2 * P + 1), s));
+    std::vector<unsigned long long> h(1 + P);
+    cudaError_t e = cudaMemsetAsync(d, 0, sizeof(unsigned long long) * (2 * P + 1), s);
+    if (e == cudaSuccess)
+        e = launch_partition_hist(cols, rows, false, 0, 0, key_col, radix_shift, radix_bits, d, s, ctx);
+    if (e == cudaSuccess) e = launch_partition_cursors(d, radix_bits, d + P, out_stride, s, ctx);
+    if (e == cudaSuccess)
+        e = launch_partition_scatter(cols, ncols, rows, false, 0, 0, key_col, radix_shift, radix_bits, d, out,
+                                     out_stride, s, ctx);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), d + P, sizeof(unsigned long long) * (1 + P), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(d, s);
+    if (e != cudaSuccess) return cuda_fail(e, "mgv_partition_columns");
+    const mgv_status st = check_device(ctx, s);
+    if (st != MGV_OK) return st;
+    for (uint32_t p = 0; p < P; ++p) counts[p] = h[1 + p];
+    return MGV_OK;
+}
+
 // Host ingest: slices of the host columns go through `depth` pool buffers;
 // the copy stream fills buffer k % depth once its previous slice has been
 // consumed, and the consume of slice k waits for its copy only.

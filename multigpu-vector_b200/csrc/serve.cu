@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -71,6 +72,8 @@ struct Inflight {
     std::vector<std::shared_ptr<Request>> reqs;
     void* dmem = nullptr;    // the slot's device region, kept and grown on demand
     size_t dmem_cap = 0;
+    unsigned char* hdesc = nullptr;  // pinned staging of the batch's descriptors: one copy per launch
+    size_t hdesc_cap = 0;
     size_t charge = 0;
     Landing* land = nullptr;          // where this batch's results land
     std::vector<uint64_t> offs;
@@ -126,6 +129,9 @@ void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
 }
 
 constexpr uint64_t kMinLandingRows = 1u << 18;  // 6 MiB of group rows
+// Pending requests an idle server still answers one at a time (oldest first)
+// through the single-query chain; a longer queue is batched.
+constexpr size_t kSoloBacklog = 2;
 
 // A free landing zone of at least `rows` rows and `ncounts` counts (scheduler
 // thread, lock not held; the list is read and changed under the lock, a new
@@ -257,13 +263,24 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
                          reinterpret_cast<uint32_t*>(A + counts_off) + i, r.max_groups, 0};
     }
     cudaStream_t s = sl.stream;
-    // host staging of descriptors must outlive the copies: pageable copies
-    // are staged by the driver before cudaMemcpyAsync returns
-    MGV_CUDA_TRY(cudaMemcpyAsync(A + qs_off, hq.data(), sizeof(ChainDev) * nq, cudaMemcpyHostToDevice, s));
-    MGV_CUDA_TRY(cudaMemcpyAsync(A + outs_off, ho.data(), sizeof(BatchOut) * nq, cudaMemcpyHostToDevice, s));
-    if (!pi.empty())
-        MGV_CUDA_TRY(cudaMemcpyAsync(A + pi_off, pi.data(), sizeof(BatchItem) * pi.size(), cudaMemcpyHostToDevice, s));
-    MGV_CUDA_TRY(cudaMemcpyAsync(A + ci_off, ci.data(), sizeof(BatchItem) * ci.size(), cudaMemcpyHostToDevice, s));
+    // The descriptors [qs | outs | probe items | compact items] are laid out
+    // on the device as in the slot's pinned staging area and go over in one
+    // copy.  The staging stays untouched until the slot's batch has
+    // completed (a busy slot is never launched on).
+    const size_t desc_bytes = off - qs_off;
+    if (desc_bytes > sl.hdesc_cap) {
+        if (sl.hdesc) MGV_CUDA_TRY(cudaFreeHost(sl.hdesc));
+        sl.hdesc = nullptr;
+        sl.hdesc_cap = 0;
+        const size_t cap = desc_bytes + desc_bytes / 2 + 4096;
+        MGV_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&sl.hdesc), cap));
+        sl.hdesc_cap = cap;
+    }
+    std::memcpy(sl.hdesc + (qs_off - qs_off), hq.data(), sizeof(ChainDev) * nq);
+    std::memcpy(sl.hdesc + (outs_off - qs_off), ho.data(), sizeof(BatchOut) * nq);
+    if (!pi.empty()) std::memcpy(sl.hdesc + (pi_off - qs_off), pi.data(), sizeof(BatchItem) * pi.size());
+    std::memcpy(sl.hdesc + (ci_off - qs_off), ci.data(), sizeof(BatchItem) * ci.size());
+    MGV_CUDA_TRY(cudaMemcpyAsync(A + qs_off, sl.hdesc, desc_bytes, cudaMemcpyHostToDevice, s));
     MGV_CUDA_TRY(launch_fill_i32(reinterpret_cast<int32_t*>(A), slots, kEmptyKey, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(A + zero_begin, 0, zero_end - zero_begin, s));
     MGV_CUDA_TRY(cudaMemsetAsync(A + counts_off, 0, 4ull * nq, s));
@@ -373,11 +390,13 @@ void scheduler(mgv_server* S) {
         for (auto& sl : S->slots)
             if (!sl.busy) { free_slot = &sl; break; }
         const size_t budget = S->cfg.memory_budget > S->table_bytes ? S->cfg.memory_budget - S->table_bytes : 0;
-        if (!any_busy && !S->cfg.batch_solo && S->pending.size() == 1 &&
+        if (!any_busy && !S->cfg.batch_solo && !S->pending.empty() && S->pending.size() <= kSoloBacklog &&
             S->used + S->pending.front()->bytes <= budget) {
-            // a lone request on an idle server: the single-query chain answers
-            // it without batch planning or event polling (admitted and charged
-            // like a batch of one)
+            // a short queue on an idle server: the oldest request runs alone
+            // through the single-query chain, without batch planning or event
+            // polling (admitted and charged like a batch of one); batches form
+            // only once a backlog builds up, where running requests together
+            // shortens the queue
             auto q = S->pending.front();
             S->pending.pop_front();
             S->used += q->bytes;
@@ -432,7 +451,7 @@ void scheduler(mgv_server* S) {
         }
         if (S->stop && S->pending.empty() && !any_busy) break;
         if (any_busy)
-            S->cv.wait_for(lk, std::chrono::microseconds(20));  // poll the GPU
+            S->cv.wait_for(lk, std::chrono::microseconds(5));  // poll the GPU
         else
             S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
     }
@@ -609,6 +628,7 @@ mgv_status mgv_server_destroy(mgv_server* S) {
     for (auto& sl : S->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         if (sl.dmem) cudaFree(sl.dmem);
+        if (sl.hdesc) cudaFreeHost(sl.hdesc);
         if (sl.done) cudaEventDestroy(sl.done);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }

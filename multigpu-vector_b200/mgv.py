@@ -235,6 +235,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                        c_void_p, c_void_p]),
         "mgv_diag_random_gather": (st, [c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, POINTER(c_double)]),
         "mgv_pool_device_get": (st, [c_void_p, POINTER(PoolDevice)]),
+        "mgv_partition_columns": (st, [c_void_p, POINTER(c_void_p), c_uint32, c_uint64, c_uint32, c_uint32, c_uint32,
+                                       c_void_p, c_uint64, POINTER(c_uint64), c_void_p]),
         "mgv_op_consume_host": (st, [c_void_p, c_void_p, POINTER(c_void_p), c_uint32, c_uint64, c_void_p]),
         "mgv_diag_gather": (st, [c_void_p, POINTER(DiagGatherDesc), POINTER(c_double)]),
         "mgv_gen_zipf": (st, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_uint32, c_double, c_void_p]),
@@ -330,6 +332,16 @@ class Context:
         ms = c_double()
         _call("mgv_diag_gather", self.h, byref(d), byref(ms))
         return ms.value
+
+    def partition_columns(self, cols, rows: int, key_col: int, radix_bits: int, radix_shift: int, out,
+                          out_stride: int, stream=None) -> list[int]:
+        """mgv_partition_columns: rows of device columns written partition-major into
+        `out` (column c at out + c * out_stride); returns the rows per partition."""
+        arr = (c_void_p * max(1, len(cols)))(*[_ptr(c) for c in cols])
+        counts = (c_uint64 * (1 << radix_bits))()
+        _call("mgv_partition_columns", self.h, arr, len(cols), rows, key_col, radix_bits, radix_shift,
+              c_void_p(_ptr(out)), out_stride, counts, _stream(stream))
+        return list(counts)
 
     # seeded columns ---------------------------------------------------
     def gen_uniform(self, dst, n, seed, stream_id, lo, rng, stream=None):
