@@ -1188,11 +1188,11 @@ mgv_status mgv_op_consume_host(mgv_op* o, mgv_pool* pool, const int32_t* const* 
     if (!o || !pool || (!host_cols && ncols)) return fail(MGV_EINVAL, "NULL argument");
     if (ncols == 0 || ncols > MGV_MAX_COLS || ncols > pool->ncols)
         return fail(MGV_EINVAL, "column count must be 1..the pool's columns");
-    for (uint32_t c = 0; c < ncols; ++c)
-        if (!host_cols[c]) return fail(MGV_EINVAL, "host column is NULL");
     if (pool->ctx->device != o->ctx->device) return fail(MGV_EINVAL, "pool and operator on different devices");
     if (!all_open(o)) return fail(MGV_ESTATE, "chain is not open");
     if (rows == 0) return MGV_OK;
+    for (uint32_t c = 0; c < ncols; ++c)
+        if (!host_cols[c]) return fail(MGV_EINVAL, "host column is NULL");
     MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
     cudaStream_t s = pick_stream(o->ctx, stream);
     if (!o->in_stream) {
