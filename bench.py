@@ -357,12 +357,21 @@ def main():
         assert want == (cnt, s), f"join result {(cnt, s)} differs from the oracle's {want}"
         checked = f"oracle: COUNT and SUM equal the oracle's chained-table join over all {npb} probe rows"
         cpu = cpu_probe_baseline(chain, hpk, hpp, args.cpu_sample, threads)
+    # ---- the probe's own ceiling: random 32-byte reads of a table this size (N = 1) ----
+    ceiling = None
+    if world == 1 and not args.no_extras:
+        ms = ctx.diag_gather(int(info.table_bytes), npb, line_bytes=32, method=0, ctas_per_sm=2, reps=5, inflight=4,
+                             lsu_warps=8)
+        ceiling = {"what": "random 32-byte bucket reads of a table of this size with nothing else in the kernel "
+                           "(mgv_diag_gather, LSU, 2 CTAs x 8 warps per SM, 4 reads in flight per lane)",
+                   "lookups_per_s": npb / (ms / 1e3), "probe_tuples_per_s": npb / kernel_s,
+                   "frac": (npb / kernel_s) / (npb / (ms / 1e3))}
     # ---- the metric's other half: batched and served queries vs plain (N = 1) ----
     extras = {}
     if world == 1 and not args.no_extras:
         extras = run_extras(args, mgv, torch, ctx)
     return finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank,
-                  dist, (probe, agg, bhead, hb), nb, npb, tuning, extras, checked)
+                  dist, (probe, agg, bhead, hb), nb, npb, tuning, extras, checked, ceiling)
 
 
 def run_extras(args, mgv, torch, ctx):
@@ -462,7 +471,7 @@ def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world,
 
 
 def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank, dist,
-           ops, nb, npb, tuning, extras=None, checked=None):
+           ops, nb, npb, tuning, extras=None, checked=None, ceiling=None):
     import replicas
 
     value = replicas.job_rate(world, npb * args.steps, elapsed)
@@ -485,7 +494,7 @@ def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, 
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "kernel_ms": kernel_s * 1000.0,
                      "algorithmic_bytes_per_launch": BYTES_PER_TUPLE * npb,
-                     "traffic": probe_traffic_per_launch()},
+                     "traffic": probe_traffic_per_launch(), "lookup_ceiling": ceiling},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,

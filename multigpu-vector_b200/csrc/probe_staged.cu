@@ -58,6 +58,14 @@ struct ContQueue {
 
 __device__ __forceinline__ uint32_t next_bucket(uint32_t b, uint32_t nb) { return (b + 1 == nb) ? 0u : b + 1; }
 
+// Home bucket of a key: the radix-laid-out form (RADIX), or the plain
+// multiply-shift of the hash for an unpartitioned table (fewer instructions
+// per probe on the common path).
+template <bool RADIX>
+__device__ __forceinline__ uint32_t home(int32_t key, const TableView& t) {
+    return RADIX ? home_bucket(key, t) : __umulhi(murmur32((uint32_t)key), t.nbuckets);
+}
+
 // Fold one bucket's matches for (key, pay); returns whether the run goes on.
 template <bool UNIQUE, bool ADD_BP, bool ADD_PP>
 __device__ __forceinline__ bool fold(const uint32_t (&w)[8], int32_t key, int32_t pay, Acc& a) {
@@ -110,7 +118,7 @@ __device__ __forceinline__ void fold_reserved(const TableView& t, int32_t pay, A
 // to issue the bucket loads and again to fold the results -- so that no
 // key or payload stays in a register across the L2 latency.  Returns a
 // value that depends on every row read (for releasing a stage safely).
-template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
 __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, uint32_t valid, ContQueue& q,
                                           bool drain, const TableView& t, Acc& a) {
     const uint32_t lane = lane_id();
@@ -134,7 +142,7 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
     uint32_t w[R][8];
 #pragma unroll
     for (int r = 0; r < R; ++r)
-        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * home_bucket(rk[32 * r], t), w[r]);
+        if ((valid >> r) & 1u) ld_bucket(t.slots + 4ull * home<RADIX>(rk[32 * r], t), w[r]);
     uint32_t wc[8];
     if (has_c) ld_bucket(t.slots + 4ull * cb, wc);
     __syncwarp();  // every lane has read its queue entry before anyone appends
@@ -149,7 +157,7 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
         if (key == kEmptyKey) {
             fold_reserved<ADD_BP, ADD_PP>(t, pay, a);
         } else if (fold<UNIQUE, ADD_BP, ADD_PP>(w[r], key, pay, a)) {
-            enqueue<Q>(q, key, pay, next_bucket(home_bucket(key, t), t.nbuckets));
+            enqueue<Q>(q, key, pay, next_bucket(home<RADIX>(key, t), t.nbuckets));
         }
     }
     if (has_c && fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a)) enqueue<Q>(q, ck, cp, next_bucket(cb, t.nbuckets));
@@ -158,16 +166,16 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
 
 // Continuation-only rounds until a full round can no longer overflow the
 // queue.  They never grow it, and every run ends, so this terminates.
-template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
 __device__ __forceinline__ void make_room(ContQueue& q, const TableView& t, Acc& a, uint32_t limit) {
     for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
         __syncwarp();
         if (*((volatile uint32_t*)q.tail) - q.head <= limit) break;
-        round<R, Q, UNIQUE, ADD_BP, ADD_PP>(nullptr, nullptr, 0u, q, true, t, a);
+        round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(nullptr, nullptr, 0u, q, true, t, a);
     }
 }
 
-template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
 __global__ void __launch_bounds__(kThreads, MB)
     k_probe_agg_ws(const int32_t* __restrict__ keys, const int32_t* __restrict__ pays, uint64_t n, TableView t,
                    unsigned long long* acc, uint32_t* err) {
@@ -239,8 +247,8 @@ __global__ void __launch_bounds__(kThreads, MB)
                 if (lane == 0) set_error(err, kDevTimeout, 12);
                 break;
             }
-            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
-            const uint32_t dep = round<R, Q, UNIQUE, ADD_BP, ADD_PP>(sk + s * T + row0, sp + s * T + row0,
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, kRoomLimit);
+            const uint32_t dep = round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(sk + s * T + row0, sp + s * T + row0,
                                                                      (1u << R) - 1u, q, false, t, a);
             // Release the stage once every lane's reads of it have landed:
             // combine the values read across the warp (the reduction waits
@@ -260,19 +268,19 @@ __global__ void __launch_bounds__(kThreads, MB)
             uint32_t valid = 0;
 #pragma unroll
             for (int r = 0; r < R; ++r) valid |= (uint32_t)(base + 32 * r < n) << r;
-            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, kRoomLimit);
-            round<R, Q, UNIQUE, ADD_BP, ADD_PP>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false, t, a);
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, kRoomLimit);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false, t, a);
         }
         // drain the continuation queue
-        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP>(q, t, a, 0u);
+        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, 0u);
     }
     block_accumulate2<kThreads>((unsigned long long)a.cnt, a.sum, acc);
 }
 
-template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP>
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
 cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
                      unsigned long long* acc, int ctas_per_sm, cudaStream_t s, Context* ctx) {
-    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP>;
+    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX>;
     constexpr int T = kConsumerWarps * 32 * R;
     const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
                         (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) +
@@ -292,15 +300,22 @@ cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const
     return cudaGetLastError();
 }
 
+template <int R, int S, int MB, bool UNIQUE, bool RADIX>
+cudaError_t launch_mode_r(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t, uint32_t mode,
+                          unsigned long long* acc, int ctas, cudaStream_t s, Context* ctx) {
+    switch (mode) {
+        case 0: return launch_v<R, S, MB, UNIQUE, false, false, RADIX>(keys, pays, n, t, acc, ctas, s, ctx);
+        case 1: return launch_v<R, S, MB, UNIQUE, true, false, RADIX>(keys, pays, n, t, acc, ctas, s, ctx);
+        case 2: return launch_v<R, S, MB, UNIQUE, false, true, RADIX>(keys, pays, n, t, acc, ctas, s, ctx);
+        default: return launch_v<R, S, MB, UNIQUE, true, true, RADIX>(keys, pays, n, t, acc, ctas, s, ctx);
+    }
+}
+
 template <int R, int S, int MB, bool UNIQUE>
 cudaError_t launch_mode(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t, uint32_t mode,
                         unsigned long long* acc, int ctas, cudaStream_t s, Context* ctx) {
-    switch (mode) {
-        case 0: return launch_v<R, S, MB, UNIQUE, false, false>(keys, pays, n, t, acc, ctas, s, ctx);
-        case 1: return launch_v<R, S, MB, UNIQUE, true, false>(keys, pays, n, t, acc, ctas, s, ctx);
-        case 2: return launch_v<R, S, MB, UNIQUE, false, true>(keys, pays, n, t, acc, ctas, s, ctx);
-        default: return launch_v<R, S, MB, UNIQUE, true, true>(keys, pays, n, t, acc, ctas, s, ctx);
-    }
+    if (t.radix_mask != 0) return launch_mode_r<R, S, MB, UNIQUE, true>(keys, pays, n, t, mode, acc, ctas, s, ctx);
+    return launch_mode_r<R, S, MB, UNIQUE, false>(keys, pays, n, t, mode, acc, ctas, s, ctx);
 }
 
 }  // namespace

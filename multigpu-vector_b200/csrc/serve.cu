@@ -451,7 +451,7 @@ void scheduler(mgv_server* S) {
         }
         if (S->stop && S->pending.empty() && !any_busy) break;
         if (any_busy)
-            S->cv.wait_for(lk, std::chrono::microseconds(5));  // poll the GPU
+            S->cv.wait_for(lk, std::chrono::microseconds(20));  // poll the GPU
         else
             S->cv.wait(lk, [&] { return S->stop || !S->pending.empty(); });
     }
