@@ -161,6 +161,40 @@ def cpu_probe_baseline(chain, pk, pp, sample, threads):
                                     "(ours: the loop split over the host's threads)"}}
 
 
+def run_gather(args, mgv):
+    """Random-read ceilings of this GPU (include/mgv_diag.h), one JSON line."""
+    ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    if args.gather_once:
+        ms = ctx.diag_gather(args.gather_once << 20, 1 << 24, line_bytes=32, method=0, ctas_per_sm=2, reps=1,
+                             inflight=4, lsu_warps=8)
+        print(json.dumps({"gather_once": {"table_mib": args.gather_once, "lookups": 1 << 24, "ms": ms}}), flush=True)
+        ctx.close()
+        return 0
+    n = 1 << 26
+    out = []
+
+    def one(**kw):
+        try:
+            ms = ctx.diag_gather(lookups=n, reps=10, **kw)
+            out.append(dict(kw, ms=ms, g_lookups_per_s=n / ms / 1e6))
+        except mgv.MgvError as e:
+            out.append(dict(kw, error=str(e)))
+
+    for mib in (40, 80):
+        for lb in (32, 64, 128):
+            for c in (2, 4):
+                one(table_bytes=mib << 20, line_bytes=lb, method=0, ctas_per_sm=c, inflight=4, lsu_warps=8)
+    for lb in (32, 64):
+        for tw in (1, 2, 4):
+            one(table_bytes=40 << 20, line_bytes=lb, method=1, ctas_per_sm=2, inflight=2, tma_warps=tw)
+    for sh in (0.1, 0.2, 0.35):
+        one(table_bytes=40 << 20, line_bytes=32, method=2, ctas_per_sm=2, inflight=4, lsu_warps=8, tma_warps=1,
+            tma_share=sh)
+    print(json.dumps({"gather_ceiling": out, "lookups": n}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -217,8 +251,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and served summaries added to the join line (N = 1)")
-    ap.add_argument("--load-factor", type=float, default=0.4,
-                    help="join table load factor; 0.4 (an 80 MiB table for 2^22 keys) measured fastest")
+    ap.add_argument("--load-factor", type=float, default=0.45,
+                    help="join table load factor; 0.45 (a 71 MiB table for 2^22 keys) measured fastest under sustained "
+                         "load (0.4 reads more of the table from DRAM and draws the GPU into its power cap; 0.5 and "
+                         "up continue more runs into a second bucket)")
     ap.add_argument("--pipeline-load-factor", type=float, default=0.4,
                     help="pipeline: load factor of the 2^24-key radix-partitioned table (0.4 measured fastest)")
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
@@ -233,11 +269,16 @@ def main():
     ap.add_argument("--queries", type=int, default=512, help="batched: queries in the mix")
     ap.add_argument("--batch-config", default=None,
                     help="batched: 'load_factor,probe_item_rows,item_order' instead of autotuning")
-    ap.add_argument("--serve-seconds", type=float, default=1.0, help="served: arrival window per rate")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="served: arrival window per rate")
     ap.add_argument("--rates", default="200,1000,5000", help="served: arrival rates (queries/s)")
+    ap.add_argument("--served-plain-first", action="store_true",
+                    help="served: run the plain server before the batched one at each rate")
     ap.add_argument("--saturate", type=int, default=5000, help="served: requests in the closing burst")
     ap.add_argument("--gather-ceiling", action="store_true",
-                    help="measure the random 32-byte bucket-read ceiling instead of the join")
+                    help="measure the random bucket-read ceilings (line widths 32/64/128 B, LSU and TMA gather4, "
+                         "40 and 80 MiB tables) instead of the join")
+    ap.add_argument("--gather-once", type=int, default=0, metavar="MIB",
+                    help="one 32-byte LSU gather pass set over a table of MIB MiB (2^24 lookups; for ncu captures)")
     ap.add_argument("--settle-s", type=float, default=1.0, help="untimed steps before timing, in seconds")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -252,17 +293,8 @@ def main():
         import workloads
 
         return workloads.run(args)
-    if args.gather_ceiling:
-        ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
-        out = []
-        for tb in (1 << 20, 32 << 20, 64 << 20):
-            for c in (2, 4):
-                ms = ctx.diag_random_gather(tb, args.probe_rows, c, 20)
-                out.append({"table_bytes": tb, "ctas_per_sm": c, "ms_per_pass": ms,
-                            "gather_per_s": args.probe_rows / (ms / 1e3)})
-        print(json.dumps({"gather_ceiling": out, "rows": args.probe_rows}), flush=True)
-        ctx.close()
-        return 0
+    if args.gather_ceiling or args.gather_once:
+        return run_gather(args, mgv)
 
     import replicas
 
@@ -484,8 +516,8 @@ def finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, 
         "config": {
             "workload": WORKLOAD, "build_rows": nb, "probe_rows": npb, "load_factor": args.load_factor,
             "table_bytes": int(info.table_bytes), "build_ms": build_ms, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2: 512 MiB of probe columns streamed per step; the hash table "
-                  "stays L2-resident by design",
+            "l2": "inputs larger than L2: 512 MiB of probe columns streamed per step (evict-first); the hash "
+                  "table is read at random and about half to two thirds of its sectors hit in L2",
             "step": "open -> consume(2^26 rows) -> close (COUNT + SUM read back)",
             "tuning": {"probe_kernel": tuning.probe_kernel, "rows_per_thread": tuning.probe_rows_per_thread,
                        "stages": tuning.probe_stages, "ctas_per_sm": tuning.probe_ctas_per_sm},

@@ -92,7 +92,9 @@ typedef struct mgv_tuning {
     float default_load_factor;      /* hash_build tables whose desc gives 0            */
     uint32_t groupby_smem_slots;    /* largest per-CTA shared group table: 0 (off) or a
                                        power of 2 in [64, 8192]; default 8192        */
-    uint32_t reserved[2];
+    uint32_t select_ctas_per_sm;    /* select -> aggregate kernel: CTAs of 256 threads
+                                       per SM, 1..8 (0 = the default, 2)             */
+    uint32_t reserved;
 } mgv_tuning;
 
 mgv_status mgv_ctx_set_tuning(mgv_ctx *ctx, const mgv_tuning *t);

@@ -263,6 +263,7 @@ mgv_status mgv_ctx_set_tuning(mgv_ctx* ctx, const mgv_tuning* t) {
     const uint32_t gs = t->groupby_smem_slots;
     if (gs != 0 && (gs < 64 || gs > kMaxSmemGroups || (gs & (gs - 1)) != 0))
         return fail(MGV_EINVAL, "groupby_smem_slots must be 0 or a power of two in [64, 8192]");
+    if (t->select_ctas_per_sm > 8) return fail(MGV_EINVAL, "select_ctas_per_sm must be 0..8");
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuning = *t;
     return MGV_OK;

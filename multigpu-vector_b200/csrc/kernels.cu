@@ -115,9 +115,10 @@ static cudaError_t select_agg_v(const int32_t* f, int32_t bound, const int32_t* 
     const bool vec = aligned32(f) && aligned32(a) && aligned32(b);
     const void* k = vec ? (const void*)k_select_agg<SEL, HASA, HASB, true>
                         : (const void*)k_select_agg<SEL, HASA, HASB, false>;
-    // two CTAs per SM: enough loads in flight to fill HBM, and few CTAs adding
-    // into the one accumulator (same-address atomics serialise in L2)
-    int grid = std::min(occupancy_grid(k, kBlock, 0, ctx), 2 * ctx->prop.multiProcessorCount);
+    // two CTAs per SM by default: enough loads in flight to fill HBM, and few
+    // CTAs adding into the one accumulator (same-address atomics serialise in L2)
+    const int per_sm = ctx->tuning.select_ctas_per_sm ? (int)ctx->tuning.select_ctas_per_sm : 2;
+    int grid = std::min(occupancy_grid(k, kBlock, 0, ctx), per_sm * ctx->prop.multiProcessorCount);
     uint64_t need = (n / 8 + kBlock - 1) / kBlock + 1;
     if ((uint64_t)grid > need) grid = (int)need;
     if (vec)

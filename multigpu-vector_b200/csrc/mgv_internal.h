@@ -115,7 +115,7 @@ struct Context {
     // pinned landing zone for close(): [0..1] error word, [2..] result words
     unsigned long long* h_stage = nullptr;
     std::atomic<uint64_t> launches{0};
-    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, kMaxSmemGroups, {0u, 0u}};
+    mgv_tuning tuning{0u, 4u, 4u, 3u, 0.5f, kMaxSmemGroups, 0u, 0u};
     mgv_batch_config batch_tuned{};  // the batch autotuner's last choice
     bool has_batch_tuned = false;
     std::mutex mu;

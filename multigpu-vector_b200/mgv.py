@@ -55,7 +55,7 @@ class CtxInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("probe_kernel", c_uint32), ("probe_rows_per_thread", c_uint32), ("probe_stages", c_uint32),
                 ("probe_ctas_per_sm", c_uint32), ("default_load_factor", c_float),
-                ("groupby_smem_slots", c_uint32), ("reserved", c_uint32 * 2)]
+                ("groupby_smem_slots", c_uint32), ("select_ctas_per_sm", c_uint32), ("reserved", c_uint32)]
 
 
 class PoolStats(ctypes.Structure):

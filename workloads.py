@@ -89,9 +89,12 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     with torch.cuda.stream(stream):
         c0 = torch.empty(n, dtype=torch.int32, device="cuda")
         c1 = torch.empty(n, dtype=torch.int32, device="cuda")
-        # 1 GiB > L2; its fill also outlasts the host's enqueueing of open and
+        # 1 GiB > L2, read (not written) between steps: a written flush would
+        # leave the L2 full of dirty lines whose write-back the next kernel
+        # pays for; the read also outlasts the host's enqueueing of open and
         # consume, so the kernel's events see the kernel, not a launch gap
-        flush = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+        flush = torch.ones(1 << 27, dtype=torch.int64, device="cuda")
+        flush_out = torch.empty((), dtype=torch.int64, device="cuda")
     ctx.gen_uniform(c0, n, 0x5EED0001, 0, 0, 1 << 31, stream=stream)
     ctx.gen_uniform(c1, n, 0x5EED0001, 1, 0, 1 << 20, stream=stream)
     head, agg = mgv.create_sum_select_pipeline(ctx, bound, 0, 1)
@@ -100,7 +103,7 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     h0 = time.time()
     for i in range(args.warmup + args.steps):
         with torch.cuda.stream(stream):
-            flush.fill_(i & 0xFF)  # inputs come from HBM every step
+            torch.sum(flush, dim=0, out=flush_out)  # inputs come from HBM every step
         e0, e1 = _events(torch)
         k0, k1 = _events(torch)
         e0.record(stream)
@@ -117,7 +120,7 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     clk.mark(h0, time.time())
     launches = (ctx.launches - launches0) * args.steps // (args.warmup + args.steps)
     cnt, s = agg.result()
-    del flush
+    del flush, flush_out
     t = statistics.median(times)
     kt = statistics.median(ktimes)
     peak, kind = bench.measured_peaks()
@@ -129,7 +132,7 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     h0c, h1c = c0.cpu().pin_memory(), c1.cpu().pin_memory()
     pool = mgv.Pool(ctx, 3, 1 << 20, 2)
     et = []
-    for i in range(3 + max(3, args.steps // 4)):
+    for i in range(3 + max(10, args.steps)):
         e0, e1 = _events(torch)
         e0.record(stream)
         head.open(stream)
@@ -146,7 +149,8 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     hb = torch.cat([h0c, h1c]).pin_memory()
     h2d = _h2d_gbs(torch, hb, both, stream)
     pool.destroy()
-    workload = "select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between steps"
+    workload = ("select c0 < 2^30 over 2^22 rows (c0 U[0,2^31)), COUNT + int64 SUM(c1 U[0,2^20)); L2 flushed between "
+                "steps by reading 1 GiB")
     extra = {"roofline": {"bound": "hbm", "achieved": 8 * n / kt / 1e9, "peak": peak, "unit": "GB/s",
                           "frac": 8 * n / kt / 1e9 / peak, "peak_kind": kind, "kernel_ms": 1000 * kt,
                           "algorithmic_bytes_per_launch": 8 * n, "kernel": "k_select_agg"},
@@ -484,6 +488,10 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
             st = mgv.load().mgv_server_wait(srv.h, tk, 600000, wbuf, 1 << 16, ctypes.byref(wn), ctypes.byref(wlat))
             assert st == mgv.OK
         srv.reset_stats()
+        # both servers start their timed window from an idle GPU: the batched
+        # warm-up burst runs the GPU flat out, and its power-capped clocks
+        # would otherwise still be recovering at the first timed requests
+        time.sleep(0.5)
         at, reqs = trace(rate, seed)
         # Results are drained by a second thread while requests arrive (the
         # ctypes wait releases the GIL).  It only waits: request i's rows land
@@ -548,8 +556,12 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
     out = []
     h0 = time.time()
     for k, rate in enumerate(rates + [0.0]):
-        b, rb = serve(False, rate, 1000 + k)
-        p, rp = serve(True, rate, 1000 + k)
+        if getattr(args, "served_plain_first", False):
+            p, rp = serve(True, rate, 1000 + k)
+            b, rb = serve(False, rate, 1000 + k)
+        else:
+            b, rb = serve(False, rate, 1000 + k)
+            p, rp = serve(True, rate, 1000 + k)
         assert rb == rp, "served results differ from the plain server"
         out.append({"rate": rate if rate else "saturated", "batched": b, "plain": p})
     clk.mark(h0, time.time())
