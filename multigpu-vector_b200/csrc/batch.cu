@@ -50,6 +50,7 @@ struct mgv_batch {
     RegionJob* d_jobs = nullptr;  // one shared-memory build job per query
     RegionScratch rsc{};
     uint32_t total_regions = 0, max_job_regions = 0;
+    uint32_t key_only = 0;  // every query's build side has no payloads: 8-key buckets
     BatchOut* d_outs = nullptr;
     BatchItem* d_build_items = nullptr;
     BatchItem* d_probe_items = nullptr;
@@ -106,7 +107,9 @@ mgv_status enqueue_run(mgv_batch* b, cudaStream_t s) {
     MGV_CUDA_TRY(cudaMemsetAsync(b->group_zero, 0, b->group_zero_bytes, s));
     MGV_CUDA_TRY(cudaMemsetAsync(b->out_counts, 0, sizeof(uint32_t) * b->q.size(), s));
     // every region of every table is written by the build (no clearing pass)
-    MGV_CUDA_TRY(launch_build_regions(b->d_jobs, RegionJob{}, (uint32_t)b->q.size(), b->d_build_items, b->n_build, 0, 0,
+    RegionJob layout{};  // the jobs themselves are on the device; this carries their slot layout
+    layout.t.key_only = b->key_only;
+    MGV_CUDA_TRY(launch_build_regions(b->d_jobs, layout, (uint32_t)b->q.size(), b->d_build_items, b->n_build, 0, 0,
                                       b->total_regions, b->max_job_regions, b->rsc, true, false, s, ctx));
     MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_outs, b->d_probe_items, b->n_probe, b->d_compact_items, b->n_compact,
                               (int)b->cfg.probe_ctas_per_sm, b->cfg.item_order, s, ctx));
@@ -168,8 +171,13 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
     std::vector<size_t> t_off(nq), side_off(nq), gk_off(nq), gs_off(nq), gc_off(nq), sp_off(nq);
     const size_t tables_begin = off;
+    // one slot layout for the whole batch (one region-build launch builds every table)
+    b->key_only = 1;
+    for (uint32_t i = 0; i < nq; ++i)
+        if (qs[i].build_payloads) b->key_only = 0;
+    const double spb = b->key_only ? 8.0 : 4.0;  // slots per 32-byte bucket
     for (uint32_t i = 0; i < nq; ++i) {
-        nbk[i] = (uint32_t)std::max(1.0, std::ceil((double)std::max<uint64_t>(qs[i].build_rows, 1) / (4.0 * cfg.load_factor)));
+        nbk[i] = (uint32_t)std::max(1.0, std::ceil((double)std::max<uint64_t>(qs[i].build_rows, 1) / (spb * cfg.load_factor)));
         t_off[i] = off;
         off += (size_t)nbk[i] * 32;  // tables packed back to back: one fill clears all
     }
@@ -279,6 +287,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         t.slots = reinterpret_cast<unsigned long long*>(A + t_off[i]);
         t.nbuckets = nbk[i];
         t.bpp = nbk[i];
+        t.key_only = b->key_only;
         t.meta = b->metas + 4ull * i;
         t.side_pay = reinterpret_cast<int32_t*>(A + side_off[i]);
         t.side_cap = std::max<uint64_t>(qs[i].build_rows, 1);

@@ -320,27 +320,41 @@ __device__ __forceinline__ uint4 lds_v4(const void* p) {
     return r;
 }
 
-// The four key words of shared bucket b.
-__device__ __forceinline__ void bucket_keys(const unsigned long long* tab, uint32_t b, uint32_t (&k)[4]) {
+// Slots per bucket: 4 {key, payload} slots, or 8 keys in a key-only table.
+template <bool KO>
+constexpr uint32_t slots_per_bucket() { return KO ? 8u : 4u; }
+
+// The key words of shared bucket b (4, or 8 for a key-only table).
+template <bool KO>
+__device__ __forceinline__ void bucket_keys(const unsigned long long* tab, uint32_t b,
+                                            uint32_t (&k)[slots_per_bucket<KO>()]) {
     const uint32_t* words = reinterpret_cast<const uint32_t*>(tab) + 8 * b;
     const uint4 s01 = lds_v4(words), s23 = lds_v4(words + 4);
-    k[0] = s01.x;
-    k[1] = s01.z;
-    k[2] = s23.x;
-    k[3] = s23.z;
+    if constexpr (KO) {
+        k[0] = s01.x; k[1] = s01.y; k[2] = s01.z; k[3] = s01.w;
+        k[4] = s23.x; k[5] = s23.y; k[6] = s23.z; k[7] = s23.w;
+    } else {
+        k[0] = s01.x;
+        k[1] = s01.z;
+        k[2] = s23.x;
+        k[3] = s23.z;
+    }
 }
 
 // Inserts one staged row into the shared region.  fill[b] counts the rows
-// that asked bucket b for a slot: the first four get slots 0..3 in that order
-// (so slots fill as a prefix, as the global insert leaves them), later ones
-// move on to the next bucket.  A bucket that has turned a row away stays full,
-// so every row ends in the first bucket of its run that had room.
+// that asked bucket b for a slot: the first four (eight in a key-only table)
+// get slots 0, 1, ... in that order (so slots fill as a prefix, as the global
+// insert leaves them), later ones move on to the next bucket.  A bucket that
+// has turned a row away stays full, so every row ends in the first bucket of
+// its run that had room.
+template <bool KO>
 __device__ __forceinline__ bool region_insert(unsigned long long* tab, uint32_t* fill, uint32_t nb, uint32_t b,
                                               unsigned long long v) {
     for (; b < nb; ++b) {
         const uint32_t q = atomicAdd(fill + b, 1u);
-        if (q < 4) {
-            tab[4 * b + q] = v;
+        if (q < slots_per_bucket<KO>()) {
+            if (KO) reinterpret_cast<uint32_t*>(tab)[8 * b + q] = (uint32_t)v;  // the key alone
+            else tab[4 * b + q] = v;
             return true;
         }
     }
@@ -351,27 +365,29 @@ __device__ __forceinline__ bool region_insert(unsigned long long* tab, uint32_t*
 // itself, or in the buckets after b up to the first one that is not full.
 // Two rows with one key share their home bucket, and every bucket between
 // the two is full, so this finds every duplicate pair inside the region.
+template <bool KO>
 __device__ __forceinline__ bool bucket_has_dup(const unsigned long long* tab, const uint32_t* fill, uint32_t nb,
                                                uint32_t b) {
-    const uint32_t n = min(fill[b], 4u);
+    constexpr uint32_t S = slots_per_bucket<KO>();
+    const uint32_t n = min(fill[b], S);
     if (n < 2) return false;  // no pair in b, and b is not full
-    uint32_t k[4];
-    bucket_keys(tab, b, k);
+    uint32_t k[S];
+    bucket_keys<KO>(tab, b, k);
     bool dup = false;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < (int)S; ++i)
 #pragma unroll
-        for (int j = i + 1; j < 4; ++j) dup |= (uint32_t)j < n && k[i] == k[j];
-    if (n < 4) return dup;
+        for (int j = i + 1; j < (int)S; ++j) dup |= (uint32_t)j < n && k[i] == k[j];
+    if (n < S) return dup;
     for (uint32_t c = b + 1; c < nb && !dup; ++c) {
-        const uint32_t m = min(fill[c], 4u);
-        uint32_t o[4];
-        bucket_keys(tab, c, o);
+        const uint32_t m = min(fill[c], S);
+        uint32_t o[S];
+        bucket_keys<KO>(tab, c, o);
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < (int)S; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) dup |= (uint32_t)j < m && k[i] == o[j];
-        if (m < 4) break;
+            for (int j = 0; j < (int)S; ++j) dup |= (uint32_t)j < m && k[i] == o[j];
+        if (m < S) break;
     }
     return dup;
 }
@@ -400,6 +416,7 @@ __device__ __forceinline__ void load_region_rows(const unsigned long long* stagi
 // Regions one at a time per CTA, several CTAs per SM; the next region's
 // first rows are loaded into registers before this region's duplicate pass
 // and bulk store, so their latency overlaps that work.
+template <bool KO>
 __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJob* __restrict__ jobs, RegionJob job0,
                                                                   uint32_t njobs, uint32_t regions,
                                                                   const uint32_t* __restrict__ start,
@@ -451,11 +468,11 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
             phase ^= 1u;
             // slots fill as a prefix: a bucket's count is the index of its first empty slot
             for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) {
-                uint32_t k[4];
-                bucket_keys(tab, b, k);
+                uint32_t k[slots_per_bucket<KO>()];
+                bucket_keys<KO>(tab, b, k);
                 uint32_t n = 0;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) n += k[q] != (uint32_t)kEmptyKey;
+                for (int q = 0; q < (int)slots_per_bucket<KO>(); ++q) n += k[q] != (uint32_t)kEmptyKey;
                 fill[b] = n;
             }
         }
@@ -467,7 +484,7 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
                 const uint32_t i = i0 + u * kRBuildBlock;
                 if (i >= s1) continue;
                 const uint32_t hb = home_bucket((int32_t)(uint32_t)v[u], sj.t) - b0;
-                if (region_insert(tab, fill, nb, hb, v[u])) ++ins;
+                if (region_insert<KO>(tab, fill, nb, hb, v[u])) ++ins;
                 else ovf[atomicAdd(ovf_count, 1u)] = ((unsigned long long)j << 32) | i;  // the run leaves the region
             }
             if (i0 + kRBuildBlock * kBuildRows >= s1) break;
@@ -477,7 +494,7 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
         const uint32_t gn = next_region(g + gridDim.x, regions, start, fresh);
         if (gn < regions) load_region_rows(staging, start[gn], start[gn + 1], v);  // in flight from here on
         bool dup = false;
-        for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) dup |= bucket_has_dup(tab, fill, nb, b);
+        for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) dup |= bucket_has_dup<KO>(tab, fill, nb, b);
         fence_proxy_async_smem();  // the inserts, before the bulk store reads them
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -554,7 +571,8 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
         (e = cudaFuncSetAttribute(k_region_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
         (e = cudaFuncSetAttribute(k_region_scatter_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)wsmem)) ||
-        (e = cudaFuncSetAttribute(k_region_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)))
+        (e = cudaFuncSetAttribute(k_region_build<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)) ||
+        (e = cudaFuncSetAttribute(k_region_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)))
         return e;
     if ((e = cudaMemsetAsync(sc.hist, 0, 4ull * total_regions, s))) return e;
     if ((e = cudaMemsetAsync(sc.ovf_count, 0, 4, s))) return e;
@@ -585,10 +603,19 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
         if ((e = cudaGetLastError())) return e;
     }
     {
-        const int grid = (int)std::min<uint64_t>(
-            total_regions, (uint64_t)occupancy_grid((const void*)k_region_build, kRBuildBlock, tsmem, ctx));
-        k_region_build<<<grid, kRBuildBlock, tsmem, s>>>(d_jobs, job0, njobs, total_regions, sc.start, sc.staging,
-                                                         sc.ovf, sc.ovf_count, fresh ? 1u : 0u, ctx->d_err);
+        // every job of one launch has the same slot layout (all key-only or none)
+        const bool ko = job0.t.key_only != 0;
+        const void* kb = ko ? (const void*)k_region_build<true> : (const void*)k_region_build<false>;
+        const int grid = (int)std::min<uint64_t>(total_regions,
+                                                 (uint64_t)occupancy_grid(kb, kRBuildBlock, tsmem, ctx));
+        if (ko)
+            k_region_build<true><<<grid, kRBuildBlock, tsmem, s>>>(d_jobs, job0, njobs, total_regions, sc.start,
+                                                                   sc.staging, sc.ovf, sc.ovf_count, fresh ? 1u : 0u,
+                                                                   ctx->d_err);
+        else
+            k_region_build<false><<<grid, kRBuildBlock, tsmem, s>>>(d_jobs, job0, njobs, total_regions, sc.start,
+                                                                    sc.staging, sc.ovf, sc.ovf_count,
+                                                                    fresh ? 1u : 0u, ctx->d_err);
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     }

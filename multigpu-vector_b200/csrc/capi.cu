@@ -518,8 +518,10 @@ mgv_status mgv_op_create_hash_build(mgv_ctx* ctx, const mgv_hash_build_desc* d, 
     if (d->radix_bits > 12 || d->radix_shift > 31) return fail(MGV_EINVAL, "radix_bits <= 12, radix_shift <= 31");
     const uint64_t rows = d->expected_rows ? d->expected_rows : 1;
     const uint32_t parts = 1u << d->radix_bits;
+    // a build side without payloads keeps keys only: 8 slots per 32-byte bucket
+    const bool key_only = d->payload_col < 0;
     // buckets per region: the expected rows of one region at the load factor
-    const double bpp = std::ceil((double)rows / parts / (4.0 * lf));
+    const double bpp = std::ceil((double)rows / parts / ((key_only ? 8.0 : 4.0) * lf));
     if (bpp * parts >= 4294967295.0) return fail(MGV_EINVAL, "expected_rows too large");
     MGV_CUDA_TRY(cudaSetDevice(ctx->device));
     mgv_op* o = new_op(ctx, OpKind::HashBuild);
@@ -531,6 +533,7 @@ mgv_status mgv_op_create_hash_build(mgv_ctx* ctx, const mgv_hash_build_desc* d, 
     t.radix_shift = d->radix_shift;
     t.radix_mask = parts - 1;
     t.nbuckets = t.bpp * parts;
+    t.key_only = key_only ? 1u : 0u;
     t.side_cap = rows;
     o->table_bytes = (size_t)t.nbuckets * 32;
     mgv_status st = dev_alloc(o, (void**)&t.slots, o->table_bytes);

@@ -310,6 +310,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
     auto slot_col = [&](int c) -> const int32_t* { return a.cols[FIXED ? (c == 0 ? 0 : c + 1) : a.slot_src[c]]; };
     const uint32_t lane = lane_id();
     const uint32_t len = (uint32_t)(row_hi - row_lo);
+    const uint64_t stream_policy = l2_policy_evict_first();  // columns are read once; the join table stays
 
     // push `cnt` (<= 128) offsets of the ring starting at `start`
     auto push_vector = [&](uint32_t start, uint32_t cnt) {
@@ -328,7 +329,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
             const bool carried = (uint32_t)c < nslots;
             const int32_t* col = carried ? slot_col(c) + row_lo : nullptr;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[c][j] = (carried && in[j]) ? __ldg(col + rid[j]) : 0;
+            for (int j = 0; j < 4; ++j) v[c][j] = (carried && in[j]) ? ld_stream1(col + rid[j], stream_policy) : 0;
         }
         // value of terminal reference r for the lane's row j and build payload bp
         auto val = [&](int32_t ref, int j, int32_t bp) -> int32_t {
@@ -388,11 +389,27 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                         for (uint32_t i = 0; i < side_n; ++i) emit(r, j, a.table.side_pay[i]);
                 }
             }
+            const bool ko = a.table.key_only != 0;  // eight keys per bucket, payloads 0
             for (uint32_t round = 0; round <= nbuckets; ++round) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const uint32_t k = (uint32_t)key[j];
-                    if (unique) {  // at most one match per run
+                    if (ko) {
+                        if (unique) {  // at most one match per run
+                            bool f = false;
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) f |= live[j] && w[j][q] == k;
+                            if (__any_sync(0xffffffffu, f)) emit(f, j, 0);
+                            live[j] = live[j] && !f && w[j][7] != (uint32_t)kEmptyKey;
+                        } else {  // every match of the run
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                const bool m = live[j] && w[j][q] == k;
+                                if (__any_sync(0xffffffffu, m)) emit(m, j, 0);
+                            }
+                            live[j] = live[j] && w[j][7] != (uint32_t)kEmptyKey;
+                        }
+                    } else if (unique) {  // at most one match per run
                         bool f = false;
                         int32_t bp = 0;
 #pragma unroll
@@ -435,7 +452,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
 #pragma unroll
             for (int k = 0; k < kWinRows / 32; ++k) {
                 const uint32_t row = r0 + k * 32 + lane;
-                f[k] = row < len ? __ldg(fcol + row) : 0;
+                f[k] = row < len ? ld_stream1(fcol + row, stream_policy) : 0;
             }
         }
 #pragma unroll

@@ -61,6 +61,15 @@ __device__ __forceinline__ void ld_stream8(const int32_t* p, int32_t (&v)[8]) {
         : "l"(p));
 }
 
+// One int32 of a column read once: no L1 allocation and, with an
+// evict-first policy (l2_policy_evict_first), first-out in L2, so the
+// column's lines do not push a hash table's lines out of L2.
+__device__ __forceinline__ int32_t ld_stream1(const int32_t* p, uint64_t policy) {
+    int32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy));
+    return v;
+}
+
 // One 32-byte hash bucket (4 slots of {key, payload}), read-only during a
 // probe: kept in L2 with evict_last priority, not allocated in L1.
 __device__ __forceinline__ void ld_bucket(const unsigned long long* p, uint32_t (&w)[8]) {

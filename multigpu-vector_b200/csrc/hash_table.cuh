@@ -1,9 +1,11 @@
 // hash_table.cuh -- device logic of the open-addressing join table.
 //
 // Layout: nbuckets buckets of 32 bytes (one L2 sector), 4 slots each; a
-// slot is a 64-bit {key (low word), payload (high word)}.  The key
-// INT32_MIN marks an empty slot; build rows with that key go to a side
-// list.  A key's run starts at bucket_of(key) and continues linearly;
+// slot is a 64-bit {key (low word), payload (high word)}.  A table built
+// without payloads (key_only) holds 8 slots of a 32-bit key per bucket
+// instead: half the bytes per key, every match with payload 0.  The key
+// INT32_MIN marks an empty slot (in both layouts every 32-bit word of an
+// empty bucket is INT32_MIN); build rows with that key go to a side list.  A key's run starts at bucket_of(key) and continues linearly;
 // slots of a run are claimed in order, so a lookup may stop at the first
 // empty slot (and, for tables without duplicate keys, at the first match).
 //
@@ -32,8 +34,31 @@ __device__ __forceinline__ void table_insert(const TableView& t, int32_t key, in
         else set_error(err, kDevTableFull, 1);
         return;
     }
-    const unsigned long long v = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
     uint32_t b = home_bucket(key, t);
+    if (t.key_only) {
+        uint32_t* keys = reinterpret_cast<uint32_t*>(t.slots);
+        for (uint32_t it = 0; it < t.nbuckets; ++it) {
+            unsigned long long s[4];
+            ld_bucket_relaxed(t.slots + 4ull * b, s);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                uint32_t cur = (uint32_t)(s[j >> 1] >> (32 * (j & 1)));
+                if ((int32_t)cur == kEmptyKey) {
+                    const uint32_t old = atomicCAS(keys + 8ull * b + j, (uint32_t)kEmptyKey, (uint32_t)key);
+                    if (old == (uint32_t)kEmptyKey) {
+                        ok = true;
+                        return;
+                    }
+                    cur = old;
+                }
+                if ((int32_t)cur == key) dup = true;
+            }
+            b = (b + 1 == t.nbuckets) ? 0u : b + 1;
+        }
+        set_error(err, kDevTableFull, 2);
+        return;
+    }
+    const unsigned long long v = ((unsigned long long)(uint32_t)pay << 32) | (uint32_t)key;
     for (uint32_t it = 0; it < t.nbuckets; ++it) {
         unsigned long long s[4];
         ld_bucket_relaxed(t.slots + 4ull * b, s);
@@ -65,6 +90,16 @@ template <int R>
 __device__ __forceinline__ void table_insert_rows(const TableView& t, const int32_t (&key)[R],
                                                   const int32_t (&pay)[R], const bool (&valid)[R],
                                                   uint32_t* err, bool& dup, uint32_t& inserted) {
+    if (t.key_only) {  // key-only tables: one 32-bit claim per row (builds under 2^16 rows come here)
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            if (!valid[j]) continue;
+            bool ok;
+            table_insert(t, key[j], pay[j], err, dup, ok);
+            inserted += ok;
+        }
+        return;
+    }
     unsigned long long s[R][4];
     uint32_t b[R];
     bool fast[R];
@@ -106,12 +141,23 @@ __device__ __forceinline__ void table_insert_rows(const TableView& t, const int3
     }
 }
 
-// Matches of `key` inside one bucket w[0..7] = k0 p0 k1 p1 k2 p2 k3 p3.
-// more = the probe must continue to the next bucket.
-template <bool UNIQUE>
+// Matches of `key` inside one bucket w[0..7] = k0 p0 k1 p1 k2 p2 k3 p3
+// (KO: eight keys, every payload 0).  more = the probe must continue to the
+// next bucket.
+template <bool UNIQUE, bool KO = false>
 __device__ __forceinline__ void match_bucket(const uint32_t (&w)[8], int32_t key, uint32_t& mc,
                                              long long& ms, bool& more) {
     const uint32_t k = (uint32_t)key;
+    if (KO) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) c += w[q] == k;
+        const bool full = w[7] != (uint32_t)kEmptyKey;
+        mc = UNIQUE ? (c != 0) : c;
+        ms = 0;
+        more = UNIQUE ? (c == 0 && full) : full;
+        return;
+    }
     const bool m0 = w[0] == k, m1 = w[2] == k, m2 = w[4] == k, m3 = w[6] == k;
     const bool full = w[6] != (uint32_t)kEmptyKey;
     if (UNIQUE) {
@@ -135,7 +181,7 @@ struct Matches {
     uint32_t count;
 };
 
-template <bool UNIQUE>
+template <bool UNIQUE, bool KO = false>
 __device__ __forceinline__ Matches probe_rest(const unsigned long long* __restrict__ slots,
                                            uint32_t nbuckets, int32_t key, uint32_t b) {
     Matches r{0ull, 0u};
@@ -146,7 +192,7 @@ __device__ __forceinline__ Matches probe_rest(const unsigned long long* __restri
         uint32_t c;
         long long s;
         bool more;
-        match_bucket<UNIQUE>(w, key, c, s, more);
+        match_bucket<UNIQUE, KO>(w, key, c, s, more);
         r.count += c;
         r.sum += (unsigned long long)s;
         if (!more) break;

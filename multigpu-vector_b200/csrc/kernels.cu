@@ -215,7 +215,7 @@ cudaError_t launch_build(const int32_t* keys, const int32_t* pays, const int32_t
 // examined, so column streaming and table lookups overlap.
 // ---------------------------------------------------------------------------
 
-template <bool UNIQUE, bool VEC>
+template <bool UNIQUE, bool VEC, bool KO>
 __global__ void __launch_bounds__(kBlock, 2)
     k_probe_agg(const int32_t* __restrict__ keys, const int32_t* __restrict__ pays, uint64_t n,
                 TableView t, uint32_t sum_mode, unsigned long long* acc) {
@@ -272,9 +272,9 @@ __global__ void __launch_bounds__(kBlock, 2)
                 ms = (long long)t.meta[1];
             } else {
                 bool more;
-                match_bucket<UNIQUE>(w[r], k[r], mc, ms, more);
+                match_bucket<UNIQUE, KO>(w[r], k[r], mc, ms, more);
                 if (more) {
-                    const Matches x = probe_rest<UNIQUE>(t.slots, t.nbuckets, k[r], home_bucket(k[r], t));
+                    const Matches x = probe_rest<UNIQUE, KO>(t.slots, t.nbuckets, k[r], home_bucket(k[r], t));
                     mc += x.count;
                     ms += (long long)x.sum;
                 }
@@ -296,6 +296,12 @@ __global__ void __launch_bounds__(kBlock, 2)
     block_accumulate2<kBlock>(cnt, sum, acc);
 }
 
+template <bool KO>
+static cudaError_t probe_agg_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t, bool unique,
+                               bool vec, uint32_t sum_mode, unsigned long long* acc, cudaStream_t s, Context* ctx);
+
+// sum_mode bit 0 (add the build payload) is dropped for a key-only table:
+// its payloads are all 0.
 cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t n,
                              const TableView& t, bool unique, uint32_t sum_mode,
                              unsigned long long* acc, cudaStream_t s, Context* ctx) {
@@ -305,17 +311,24 @@ cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t 
         if (e != cudaErrorNotSupported) return e;
     }
     const bool vec = aligned32(keys) && aligned32(pays);
-    const void* k = unique ? (vec ? (const void*)k_probe_agg<true, true> : (const void*)k_probe_agg<true, false>)
-                           : (vec ? (const void*)k_probe_agg<false, true> : (const void*)k_probe_agg<false, false>);
+    if (t.key_only) return probe_agg_v<true>(keys, pays, n, t, unique, vec, sum_mode & ~1u, acc, s, ctx);
+    return probe_agg_v<false>(keys, pays, n, t, unique, vec, sum_mode, acc, s, ctx);
+}
+
+template <bool KO>
+static cudaError_t probe_agg_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t, bool unique,
+                               bool vec, uint32_t sum_mode, unsigned long long* acc, cudaStream_t s, Context* ctx) {
+    const void* k = unique ? (vec ? (const void*)k_probe_agg<true, true, KO> : (const void*)k_probe_agg<true, false, KO>)
+                           : (vec ? (const void*)k_probe_agg<false, true, KO> : (const void*)k_probe_agg<false, false, KO>);
     int grid = occupancy_grid(k, kBlock, 0, ctx);
     const uint64_t ntiles = (n + (uint64_t)kBlock * 8 - 1) / ((uint64_t)kBlock * 8);
     if ((uint64_t)grid > ntiles) grid = (int)ntiles;
     if (unique) {
-        if (vec) k_probe_agg<true, true><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
-        else k_probe_agg<true, false><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
+        if (vec) k_probe_agg<true, true, KO><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
+        else k_probe_agg<true, false, KO><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
     } else {
-        if (vec) k_probe_agg<false, true><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
-        else k_probe_agg<false, false><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
+        if (vec) k_probe_agg<false, true, KO><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
+        else k_probe_agg<false, false, KO><<<grid, kBlock, 0, s>>>(keys, pays, n, t, sum_mode, acc);
     }
     ctx->launches++;
     return cudaGetLastError();

@@ -28,8 +28,10 @@ mgv_status cuda_fail(cudaError_t e, const char* what);
 
 // ---- device views passed to kernels by value ----------------------------
 
-// Open-addressing join table: nbuckets buckets of 4 slots, each slot a
-// 64-bit {key (low word), payload (high word)}; 32-byte aligned buckets.
+// Open-addressing join table: nbuckets buckets of 32 bytes (32-byte
+// aligned), either 4 slots of 64-bit {key (low word), payload (high word)}
+// or, for a build side without payloads (key_only), 8 slots of a 32-bit key
+// (every match then has payload 0): half the bytes per key.
 struct TableView {
     unsigned long long* slots;
     uint32_t nbuckets;
@@ -40,6 +42,8 @@ struct TableView {
     uint32_t radix_shift;
     uint32_t radix_mask;
     uint32_t bpp;
+    uint32_t key_only;  // 1: 8 key slots per bucket, no payloads
+    uint32_t pad;
     // Rows whose key is the reserved empty marker INT32_MIN:
     // meta[0] = their count, meta[1] = their payload sum, meta[2] = rows
     // inserted into the table, meta[3] = duplicate-key flag.

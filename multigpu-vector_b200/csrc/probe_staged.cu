@@ -67,9 +67,20 @@ __device__ __forceinline__ uint32_t home(int32_t key, const TableView& t) {
 }
 
 // Fold one bucket's matches for (key, pay); returns whether the run goes on.
-template <bool UNIQUE, bool ADD_BP, bool ADD_PP>
+// KO: a key-only bucket of eight keys (build payloads 0, ADD_BP unused).
+template <bool UNIQUE, bool ADD_BP, bool ADD_PP, bool KO>
 __device__ __forceinline__ bool fold(const uint32_t (&w)[8], int32_t key, int32_t pay, Acc& a) {
     const uint32_t k = (uint32_t)key;
+    if (KO) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) c += w[q] == k;
+        const bool full = w[7] != (uint32_t)kEmptyKey;
+        if (UNIQUE) c = c != 0;
+        a.cnt += c;
+        if (ADD_PP) a.sum += (unsigned long long)((long long)c * pay);
+        return UNIQUE ? (c == 0 && full) : full;
+    }
     const bool m0 = w[0] == k, m1 = w[2] == k, m2 = w[4] == k, m3 = w[6] == k;
     const bool full = w[6] != (uint32_t)kEmptyKey;
     if (UNIQUE) {
@@ -118,7 +129,7 @@ __device__ __forceinline__ void fold_reserved(const TableView& t, int32_t pay, A
 // to issue the bucket loads and again to fold the results -- so that no
 // key or payload stays in a register across the L2 latency.  Returns a
 // value that depends on every row read (for releasing a stage safely).
-template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO>
 __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, uint32_t valid, ContQueue& q,
                                           bool drain, const TableView& t, Acc& a) {
     const uint32_t lane = lane_id();
@@ -156,26 +167,26 @@ __device__ __forceinline__ uint32_t round(const int32_t* rk, const int32_t* rp, 
         dep ^= (uint32_t)key ^ (uint32_t)pay;
         if (key == kEmptyKey) {
             fold_reserved<ADD_BP, ADD_PP>(t, pay, a);
-        } else if (fold<UNIQUE, ADD_BP, ADD_PP>(w[r], key, pay, a)) {
+        } else if (fold<UNIQUE, ADD_BP, ADD_PP, KO>(w[r], key, pay, a)) {
             enqueue<Q>(q, key, pay, next_bucket(home<RADIX>(key, t), t.nbuckets));
         }
     }
-    if (has_c && fold<UNIQUE, ADD_BP, ADD_PP>(wc, ck, cp, a)) enqueue<Q>(q, ck, cp, next_bucket(cb, t.nbuckets));
+    if (has_c && fold<UNIQUE, ADD_BP, ADD_PP, KO>(wc, ck, cp, a)) enqueue<Q>(q, ck, cp, next_bucket(cb, t.nbuckets));
     return dep;
 }
 
 // Continuation-only rounds until a full round can no longer overflow the
 // queue.  They never grow it, and every run ends, so this terminates.
-template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
+template <int R, int Q, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO>
 __device__ __forceinline__ void make_room(ContQueue& q, const TableView& t, Acc& a, uint32_t limit) {
     for (uint32_t guard = 0; guard < (1u << 24); ++guard) {
         __syncwarp();
         if (*((volatile uint32_t*)q.tail) - q.head <= limit) break;
-        round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(nullptr, nullptr, 0u, q, true, t, a);
+        round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(nullptr, nullptr, 0u, q, true, t, a);
     }
 }
 
-template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO = false>
 __global__ void __launch_bounds__(kThreads, MB)
     k_probe_agg_ws(const int32_t* __restrict__ keys, const int32_t* __restrict__ pays, uint64_t n, TableView t,
                    unsigned long long* acc, uint32_t* err) {
@@ -247,8 +258,8 @@ __global__ void __launch_bounds__(kThreads, MB)
                 if (lane == 0) set_error(err, kDevTimeout, 12);
                 break;
             }
-            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, kRoomLimit);
-            const uint32_t dep = round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(sk + s * T + row0, sp + s * T + row0,
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, kRoomLimit);
+            const uint32_t dep = round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(sk + s * T + row0, sp + s * T + row0,
                                                                      (1u << R) - 1u, q, false, t, a);
             // Release the stage once every lane's reads of it have landed:
             // combine the values read across the warp (the reduction waits
@@ -268,19 +279,19 @@ __global__ void __launch_bounds__(kThreads, MB)
             uint32_t valid = 0;
 #pragma unroll
             for (int r = 0; r < R; ++r) valid |= (uint32_t)(base + 32 * r < n) << r;
-            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, kRoomLimit);
-            round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false, t, a);
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, kRoomLimit);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false, t, a);
         }
         // drain the continuation queue
-        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX>(q, t, a, 0u);
+        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, 0u);
     }
     block_accumulate2<kThreads>((unsigned long long)a.cnt, a.sum, acc);
 }
 
-template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX>
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO = false>
 cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
                      unsigned long long* acc, int ctas_per_sm, cudaStream_t s, Context* ctx) {
-    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX>;
+    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>;
     constexpr int T = kConsumerWarps * 32 * R;
     const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
                         (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) +
@@ -327,6 +338,20 @@ cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, ui
                                     Context* ctx) {
     if (((uintptr_t)keys & 15u) || ((uintptr_t)pays & 15u)) return cudaErrorNotSupported;
     const uint32_t mode = (sum_mode & 1u) | ((sum_mode & 2u) && pays ? 2u : 0u);
+    if (t.key_only) {  // eight keys per bucket, payloads 0: the default shape only
+        const bool radix = t.radix_mask != 0, pp = (mode & 2u) != 0;
+        const int ctas = (int)ctx->tuning.probe_ctas_per_sm;
+#define MGV_KO(U, P, X) return launch_v<4, 4, 3, U, false, P, X, true>(keys, pays, n, t, acc, ctas, s, ctx)
+        if (unique) {
+            if (pp) { if (radix) MGV_KO(true, true, true); MGV_KO(true, true, false); }
+            if (radix) MGV_KO(true, false, true);
+            MGV_KO(true, false, false);
+        }
+        if (pp) { if (radix) MGV_KO(false, true, true); MGV_KO(false, true, false); }
+        if (radix) MGV_KO(false, false, true);
+        MGV_KO(false, false, false);
+#undef MGV_KO
+    }
     const mgv_tuning& tu = ctx->tuning;
     const int ctas = (int)tu.probe_ctas_per_sm;
     const int st = tu.probe_stages <= 2 ? 2 : tu.probe_stages <= 4 ? 4 : 6;
