@@ -463,7 +463,7 @@ typedef struct mgv_server_config {
     uint32_t max_inflight;   /* batches on the GPU at once (0 = 2, max 16)    */
     float load_factor;       /* resident join tables (0 = context default)    */
     uint32_t plain;          /* 1 = one request at a time, operator API       */
-    uint32_t batch_solo;     /* 0: while nothing is in flight and at most two
+    uint32_t batch_solo;     /* 0: while nothing is in flight and at most four
                               * requests wait, the oldest runs alone through
                               * the operator chain (lower latency); batches
                               * form once a longer queue builds up;

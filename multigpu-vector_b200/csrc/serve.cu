@@ -131,7 +131,7 @@ void complete(mgv_server* S, const std::shared_ptr<Request>& q, mgv_status st) {
 constexpr uint64_t kMinLandingRows = 1u << 18;  // 6 MiB of group rows
 // Pending requests an idle server still answers one at a time (oldest first)
 // through the single-query chain; a longer queue is batched.
-constexpr size_t kSoloBacklog = 2;
+constexpr size_t kSoloBacklog = 4;
 
 // A free landing zone of at least `rows` rows and `ncounts` counts (scheduler
 // thread, lock not held; the list is read and changed under the lock, a new
