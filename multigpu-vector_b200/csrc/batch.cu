@@ -461,7 +461,7 @@ mgv_status mgv_batch_destroy(mgv_batch* b) {
 
 mgv_status mgv_batch_autotune(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq, mgv_batch_config* out) {
     if (!ctx || (!qs && nq) || !out) return fail(MGV_EINVAL, "NULL argument");
-    const float lfs[] = {0.4f, 0.5f, 0.6f};
+    const float lfs[] = {0.4f, 0.5f, 0.6f, 0.7f, 0.8f};  // key-only tables (8 slots per bucket) take the higher ones
     const uint32_t items[] = {8192, 32768, 131072};
     const uint32_t orders[] = {0, 1};
     double best = 1e30;
