@@ -252,7 +252,7 @@ uint64_t mgv_ctx_launches(mgv_ctx* ctx) { return ctx ? ctx->launches.load() : 0;
 
 mgv_status mgv_ctx_set_tuning(mgv_ctx* ctx, const mgv_tuning* t) {
     if (!ctx || !t) return fail(MGV_EINVAL, "NULL argument");
-    if (t->probe_kernel > 2) return fail(MGV_EINVAL, "probe_kernel must be 0, 1 or 2");
+    if (t->probe_kernel > 3) return fail(MGV_EINVAL, "probe_kernel must be 0, 1, 2 or 3");
     if (t->probe_rows_per_thread != 4 && t->probe_rows_per_thread != 8)
         return fail(MGV_EINVAL, "probe_rows_per_thread must be 4 or 8");
     if (t->probe_stages != 2 && t->probe_stages != 4 && t->probe_stages != 6)

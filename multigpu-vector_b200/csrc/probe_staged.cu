@@ -288,10 +288,145 @@ __global__ void __launch_bounds__(kThreads, MB)
     block_accumulate2<kThreads>((unsigned long long)a.cnt, a.sum, acc);
 }
 
+// The same probe with the consumer rounds software-pipelined: a consumer
+// warp issues the bucket loads of its next tile row by row as it folds the
+// current tile's rows, so the register of row r is refilled right after its
+// fold and the warp always has R bucket loads in flight; the current tile's
+// stage is released once its folds are done.  Continuations are served by
+// continuation-only rounds (one load per lane) whenever the queue holds a
+// batch, which also keeps room for a tile's appends.
+template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO = false>
+__global__ void __launch_bounds__(kThreads, MB)
+    k_probe_agg_pipe(const int32_t* __restrict__ keys, const int32_t* __restrict__ pays, uint64_t n, TableView t,
+                     unsigned long long* acc, uint32_t* err) {
+    constexpr int T = kConsumerWarps * 32 * R;  // rows per tile
+    constexpr int Q = queue_len<R>();
+    constexpr uint32_t kRoomLimit = (uint32_t)(Q - 32 * (R + 1));
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    int32_t* sk = reinterpret_cast<int32_t*>(smem_raw);
+    int32_t* sp = sk + S * T;
+    int32_t* qbase = sp + (ADD_PP ? S * T : 0);
+    uint32_t* tails = reinterpret_cast<uint32_t*>(qbase + 3 * kConsumerWarps * Q);
+    uint64_t* full = reinterpret_cast<uint64_t*>(tails + kConsumerWarps);
+    uint64_t* empty = full + S;
+
+    const uint64_t nfull = n / T;
+    const uint64_t my_tiles = nfull > blockIdx.x ? (nfull - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const uint32_t tile_bytes = (uint32_t)T * sizeof(int32_t);
+    const int warp = threadIdx.x / 32;
+    const uint32_t lane = lane_id();
+    const uint32_t zero = (uint32_t)(n >> 63);  // 0 for every real row count
+
+    if (threadIdx.x < kConsumerWarps) tails[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kConsumerWarps);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    Acc a{0u, 0ull};
+    if (warp == kConsumerWarps) {
+        // ---- producer warp: keep S tiles of the probe columns in flight ----
+        if (lane == 0) {
+            const uint64_t stream_policy = l2_policy_evict_first();  // columns are read once; the table stays
+            uint64_t i = 0;
+            for (; i < my_tiles; ++i) {
+                const int s = (int)(i % S);
+                if (i >= (uint64_t)S &&
+                    !mbar_wait_bounded(&empty[s], (uint32_t)(((i / S) - 1) & 1), kWaitTries)) {
+                    set_error(err, kDevTimeout, 13);
+                    break;
+                }
+                const uint64_t tile = blockIdx.x + i * gridDim.x;
+                mbar_expect_tx(&full[s], ADD_PP ? 2 * tile_bytes : tile_bytes);
+                bulk_g2s_hint(sk + s * T, keys + tile * T, tile_bytes, &full[s], stream_policy);
+                if (ADD_PP) bulk_g2s_hint(sp + s * T, pays + tile * T, tile_bytes, &full[s], stream_policy);
+            }
+            const uint64_t lo = i > (uint64_t)S ? i - S : 0;
+            for (uint64_t j = lo; j < i; ++j) mbar_wait_bounded(&full[j % S], (uint32_t)((j / S) & 1), kWaitTries);
+        }
+    } else {
+        // ---- consumer warps ----
+        ContQueue q;
+        q.key = qbase + warp * Q;
+        q.pay = qbase + (kConsumerWarps + warp) * Q;
+        q.bucket = reinterpret_cast<uint32_t*>(qbase + (2 * kConsumerWarps + warp) * Q);
+        q.tail = tails + warp;
+        q.head = 0;
+        const int row0 = warp * 32 * R + (int)lane;
+        bool ok = true;
+        uint32_t w[R][8];
+        if (my_tiles) {
+            if (!mbar_wait_bounded(&full[0], 0u, kWaitTries)) ok = false;
+            if (__all_sync(0xffffffffu, ok)) {
+                const int32_t* rk = sk + row0;
+#pragma unroll
+                for (int r = 0; r < R; ++r) ld_bucket(t.slots + 4ull * home<RADIX>(rk[32 * r], t), w[r]);
+            } else if (lane == 0) {
+                set_error(err, kDevTimeout, 14);
+            }
+        }
+        for (uint64_t i = 0; i < my_tiles && __all_sync(0xffffffffu, ok); ++i) {
+            const int s = (int)(i % S);
+            const bool next = i + 1 < my_tiles;
+            const int s1 = (int)((i + 1) % S);
+            if (next && !mbar_wait_bounded(&full[s1], (uint32_t)(((i + 1) / S) & 1), kWaitTries)) ok = false;
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) set_error(err, kDevTimeout, 15);
+                break;
+            }
+            // room for this tile's appends; the rounds use their own registers
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, kRoomLimit);
+            const int32_t* rk = sk + s * T + row0;
+            const int32_t* rp = sp + s * T + row0;
+            const int32_t* nk = sk + s1 * T + row0;
+            uint32_t dep = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int32_t key = rk[32 * r];
+                const int32_t pay = ADD_PP ? rp[32 * r] : 0;
+                dep ^= (uint32_t)key ^ (uint32_t)pay;
+                if (key == kEmptyKey) {
+                    fold_reserved<ADD_BP, ADD_PP>(t, pay, a);
+                } else if (fold<UNIQUE, ADD_BP, ADD_PP, KO>(w[r], key, pay, a)) {
+                    enqueue<Q>(q, key, pay, next_bucket(home<RADIX>(key, t), t.nbuckets));
+                }
+                if (next) ld_bucket(t.slots + 4ull * home<RADIX>(nk[32 * r], t), w[r]);  // row r of the next tile
+            }
+            // release the stage as the plain kernel does (see k_probe_agg_ws)
+            const uint32_t wdep = __reduce_or_sync(0xffffffffu, dep);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (lane == 0) {
+                const uint32_t addr = smem_u32(&empty[s]) + ((wdep & zero) << 3);
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+            }
+        }
+        if (ok && blockIdx.x == gridDim.x - 1) {
+            // rows of the last partial tile, straight from global memory
+            const uint64_t base = nfull * T + (uint64_t)row0;
+            uint32_t valid = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) valid |= (uint32_t)(base + 32 * r < n) << r;
+            make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, kRoomLimit);
+            round<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(keys + base, ADD_PP ? pays + base : nullptr, valid, q, false,
+                                                           t, a);
+        }
+        // drain the continuation queue
+        make_room<R, Q, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>(q, t, a, 0u);
+    }
+    block_accumulate2<kThreads>((unsigned long long)a.cnt, a.sum, acc);
+}
+
 template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO = false>
 cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
                      unsigned long long* acc, int ctas_per_sm, cudaStream_t s, Context* ctx) {
-    auto k = k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>;
+    // probe_kernel 3: the software-pipelined consumer rounds
+    auto k = ctx->tuning.probe_kernel == 3 ? k_probe_agg_pipe<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>
+                                           : k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>;
     constexpr int T = kConsumerWarps * 32 * R;
     const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
                         (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) +

@@ -51,7 +51,9 @@ def config2_inputs(nb, npb, seed=0x5EED0002):
 PROBE_VARIANTS = [dict(probe_kernel=0), dict(probe_kernel=1), dict(probe_kernel=2, probe_rows_per_thread=8, probe_stages=2),
                   dict(probe_kernel=2, probe_rows_per_thread=4, probe_stages=6),
                   dict(probe_kernel=2, probe_rows_per_thread=4, probe_stages=4, probe_ctas_per_sm=3),
-                  dict(probe_kernel=2, probe_rows_per_thread=8, probe_stages=4, probe_ctas_per_sm=1)]
+                  dict(probe_kernel=2, probe_rows_per_thread=8, probe_stages=4, probe_ctas_per_sm=1),
+                  dict(probe_kernel=3, probe_rows_per_thread=4, probe_stages=4, probe_ctas_per_sm=3),
+                  dict(probe_kernel=3, probe_rows_per_thread=4, probe_stages=2, probe_ctas_per_sm=3)]
 
 
 @pytest.fixture

@@ -15,7 +15,7 @@ from gpu_util import dev, sorted_rows
 
 pytestmark = pytest.mark.gpu
 
-PROBE_VARIANTS = [dict(probe_kernel=0), dict(probe_kernel=1), dict(probe_kernel=2)]
+PROBE_VARIANTS = [dict(probe_kernel=0), dict(probe_kernel=1), dict(probe_kernel=2), dict(probe_kernel=3)]
 
 
 @pytest.fixture
