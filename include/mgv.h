@@ -84,8 +84,8 @@ uint64_t mgv_ctx_launches(mgv_ctx *ctx);
  * driver, e.g. <<<128, 1024>>> in src/main9.cu:593-594; here they are
  * runtime parameters, set by the caller or by the autotuner). */
 typedef struct mgv_tuning {
-    uint32_t probe_kernel;          /* 0 auto, 1 register prefetch, 2 bulk-copy staged,
-                                       3 staged with software-pipelined rounds        */
+    uint32_t probe_kernel;          /* 0 auto (= 3), 1 register prefetch, 2 bulk-copy
+                                       staged, 3 staged with software-pipelined rounds */
     uint32_t probe_rows_per_thread; /* staged probe: 4 or 8 rows per thread per tile   */
     uint32_t probe_stages;          /* staged probe: 2, 4 or 6 tiles in flight         */
     uint32_t probe_ctas_per_sm;     /* 0 = as many as fit; 3 with 4 rows per thread

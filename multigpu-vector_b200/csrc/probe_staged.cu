@@ -424,9 +424,10 @@ __global__ void __launch_bounds__(kThreads, MB)
 template <int R, int S, int MB, bool UNIQUE, bool ADD_BP, bool ADD_PP, bool RADIX, bool KO = false>
 cudaError_t launch_v(const int32_t* keys, const int32_t* pays, uint64_t n, const TableView& t,
                      unsigned long long* acc, int ctas_per_sm, cudaStream_t s, Context* ctx) {
-    // probe_kernel 3: the software-pipelined consumer rounds
-    auto k = ctx->tuning.probe_kernel == 3 ? k_probe_agg_pipe<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>
-                                           : k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>;
+    // probe_kernel 0 (auto) and 3: the software-pipelined consumer rounds
+    // (measured faster); 2: the plain rounds
+    auto k = ctx->tuning.probe_kernel == 2 ? k_probe_agg_ws<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>
+                                           : k_probe_agg_pipe<R, S, MB, UNIQUE, ADD_BP, ADD_PP, RADIX, KO>;
     constexpr int T = kConsumerWarps * 32 * R;
     const size_t smem = (size_t)(ADD_PP ? 2 : 1) * S * T * sizeof(int32_t) +
                         (size_t)3 * kConsumerWarps * queue_len<R>() * sizeof(int32_t) +
@@ -491,7 +492,7 @@ cudaError_t launch_probe_agg_staged(const int32_t* keys, const int32_t* pays, ui
     const int ctas = (int)tu.probe_ctas_per_sm;
     const int st = tu.probe_stages <= 2 ? 2 : tu.probe_stages <= 4 ? 4 : 6;
     // Register budgets: R = 4 at 2, 3 or 4 CTAs per SM (3 and 4 when
-    // probe_ctas_per_sm asks for them), R = 8 at 1.
+    // probe_ctas_per_sm asks for them), R = 8 at 1 (at 2 it spills).
 #define MGV_WS(RR, SS, MBB)                                                                        \
     return unique ? launch_mode<RR, SS, MBB, true>(keys, pays, n, t, mode, acc, ctas, s, ctx)     \
                   : launch_mode<RR, SS, MBB, false>(keys, pays, n, t, mode, acc, ctas, s, ctx)

@@ -481,6 +481,12 @@ mgv_status mgv_server_create(mgv_ctx* ctx, const mgv_server_config* cfg, mgv_ser
             delete S;
             return st;
         }
+        // the host rows of the class's largest result, written once now: the
+        // first request of a class then finds its pages present instead of
+        // faulting them in (a tenth of a millisecond for 65536 groups)
+        std::vector<mgv_group_row>& rows = static_cast<Op*>(gb)->gb_rows;
+        rows.resize(c);
+        rows.clear();
     }
     // landing zones pinned up front (four per in-flight slot, at most eight),
     // so serving rarely pins (slow) while batches are in flight and waiters
