@@ -255,8 +255,10 @@ def main():
                     help="join table load factor; 0.45 (a 71 MiB table for 2^22 keys) measured fastest under sustained "
                          "load (0.4 reads more of the table from DRAM and draws the GPU into its power cap; 0.5 and "
                          "up continue more runs into a second bucket)")
-    ap.add_argument("--pipeline-load-factor", type=float, default=0.4,
-                    help="pipeline: load factor of the 2^24-key radix-partitioned table (0.4 measured fastest)")
+    ap.add_argument("--pipeline-load-factor", type=float, default=0.5,
+                    help="pipeline: load factor of the 2^24-key radix-partitioned key-only table (0.5 and 0.6 "
+                         "measured fastest, 0.4 about 4 %% slower: 8 keys per bucket keep runs short at 0.5, and "
+                         "the smaller table stays in L2 more)")
     ap.add_argument("--build-rows", type=int, default=BUILD_ROWS)
     ap.add_argument("--probe-rows", type=int, default=PROBE_ROWS)
     ap.add_argument("--no-e2e", action="store_true")

@@ -720,6 +720,9 @@ static mgv_status op_reset(Op* o, cudaStream_t s) {
             break;
         case OpKind::Partition:
             o->pt_fill = 0;
+            o->pt_offered = 0;
+            o->pt_filtered = false;
+            o->pt_hist_valid = true;
             o->pt_hist.assign((size_t)1 << o->pt.radix_bits, 0);
             MGV_CUDA_TRY(cudaMemsetAsync(o->pt_acc, 0, sizeof(unsigned long long) * (o->pt_hist.size() + 1), s));
             break;
@@ -833,16 +836,25 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
         // the device's totals (and any overflow of max_rows), then the stored
         // rows -- every consume's run partition-major -- go to the parent chain;
         // a hash build on the same radix bits scatters them by sorted warp tiles
-        unsigned long long* h = o->h_res;  // [error word, rows stored, rows per partition]: one copy, one wait
-        MGV_CUDA_TRY(cudaMemcpyAsync(h, o->ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        MGV_CUDA_TRY(cudaMemcpyAsync(h + 1, o->pt_acc, sizeof(unsigned long long) * (o->pt_hist.size() + 1),
-                                     cudaMemcpyDeviceToHost, s));
-        MGV_CUDA_TRY(cudaStreamSynchronize(s));
-        const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
-        st = report_device_error(o->ctx, w, s);
-        if (st == MGV_OK) {
-            o->pt_fill = h[1];
-            for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = h[2 + p];
+        o->pt_close_stream = s;
+        if (!o->pt_filtered && o->pt_offered <= o->pt.max_rows) {
+            // every consumed row was stored: the replay needs nothing from the device, so
+            // the totals are read only if asked for (mgv_op_result) and a device error is
+            // reported by the parent's close, which waits for the stream
+            o->pt_fill = o->pt_offered;
+            o->pt_hist_valid = false;
+        } else {
+            unsigned long long* h = o->h_res;  // [error word, rows stored, rows per partition]: one copy, one wait
+            MGV_CUDA_TRY(cudaMemcpyAsync(h, o->ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaMemcpyAsync(h + 1, o->pt_acc, sizeof(unsigned long long) * (o->pt_hist.size() + 1),
+                                         cudaMemcpyDeviceToHost, s));
+            MGV_CUDA_TRY(cudaStreamSynchronize(s));
+            const uint32_t w[2] = {reinterpret_cast<uint32_t*>(h)[0], reinterpret_cast<uint32_t*>(h)[1]};
+            st = report_device_error(o->ctx, w, s);
+            if (st == MGV_OK) {
+                o->pt_fill = h[1];
+                for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = h[2 + p];
+            }
         }
         if (st == MGV_OK && o->pt_fill) {
             Op* hb = o->parent;
@@ -876,7 +888,19 @@ mgv_status mgv_op_result(mgv_op* o, void* out, size_t bytes, size_t* needed) {
             src = o->gb_rows.data();
             n = o->gb_rows.size() * sizeof(mgv_group_row);
             break;
-        case OpKind::Partition: src = o->pt_hist.data(); n = o->pt_hist.size() * sizeof(uint64_t); break;
+        case OpKind::Partition:
+            if (!o->pt_hist_valid) {  // the rows per partition, read once after the close's stream
+                MGV_CUDA_TRY(cudaSetDevice(o->ctx->device));
+                unsigned long long* h = o->h_res;
+                MGV_CUDA_TRY(cudaMemcpyAsync(h, o->pt_acc, sizeof(unsigned long long) * (o->pt_hist.size() + 1),
+                                             cudaMemcpyDeviceToHost, o->pt_close_stream));
+                MGV_CUDA_TRY(cudaStreamSynchronize(o->pt_close_stream));
+                for (size_t p = 0; p < o->pt_hist.size(); ++p) o->pt_hist[p] = h[1 + p];
+                o->pt_hist_valid = true;
+            }
+            src = o->pt_hist.data();
+            n = o->pt_hist.size() * sizeof(uint64_t);
+            break;
         default: return fail(MGV_EINVAL, "operator has no result");
     }
     if (needed) *needed = n;
@@ -985,6 +1009,8 @@ static mgv_status consume_partition(Op* part, Op* sel, const int32_t* const* col
     }
     if (ncols != part->pt_ncols) return fail(MGV_EINVAL, "partition: every consume must carry the same columns");
     if (n == 0) return MGV_OK;
+    part->pt_offered += n;
+    if (sel) part->pt_filtered = true;
     MGV_CUDA_TRY(cudaMemsetAsync(part->pt_dev, 0, sizeof(unsigned long long) * P, s));
     MGV_CUDA_TRY(launch_partition_hist(cols, n, sel != nullptr, sel ? sel->sel.col : 0, sel ? sel->sel.bound : 0,
                                        part->pt.key_col, part->pt.radix_shift, part->pt.radix_bits, part->pt_dev, s,

@@ -173,6 +173,10 @@ struct Op {
     int32_t* pt_store = nullptr;          // ncols x capacity, partition-major runs
     uint32_t pt_ncols = 0;
     uint64_t pt_fill = 0;                 // rows stored (read back at close)
+    uint64_t pt_offered = 0;              // rows consumed since open (host count)
+    bool pt_filtered = false;             // a select fed a consume: only the device knows pt_fill
+    bool pt_hist_valid = true;            // pt_hist read back (else read at mgv_op_result)
+    cudaStream_t pt_close_stream = nullptr;
     unsigned long long* pt_dev = nullptr; // [P] histogram / cursors of a consume
     unsigned long long* pt_acc = nullptr; // [1 + P] rows stored, rows per partition
     std::vector<uint64_t> pt_hist;        // rows per partition (read back at close)
