@@ -7,7 +7,8 @@
 // region by region in shared memory:
 //   1. k_region_hist     rows per region (per-CTA shared histogram per item)
 //   2. k_region_scan     exclusive prefix sum -> each region's staging range
-//   3. k_region_scatter  every row, packed {key, payload}, to its region's
+//   3. k_region_scatter  every row, packed {key, payload} (the key alone for a
+//                        key-only table), to its region's
 //                        range (per item: one global reservation per region,
 //                        then shared-memory cursors); for input already
 //                        partitioned on the table's radix bits,
@@ -55,6 +56,20 @@ __device__ __forceinline__ BatchItem item_at(const BatchItem* items, uint32_t it
     b.lo = (uint64_t)it * rpi;
     b.hi = min(n, b.lo + rpi);
     return b;
+}
+
+// Staging rows: {key, payload} as 8 bytes, or the key alone (4 bytes) for a
+// key-only table -- half the scatter's stores and the build's loads.
+template <bool KO>
+__device__ __forceinline__ void stage_put(unsigned long long* staging, uint32_t pos, unsigned long long v) {
+    if (KO) reinterpret_cast<uint32_t*>(staging)[pos] = (uint32_t)v;
+    else staging[pos] = v;
+}
+
+template <bool KO>
+__device__ __forceinline__ unsigned long long stage_get(const unsigned long long* staging, uint32_t i) {
+    if (KO) return (unsigned long long)reinterpret_cast<const uint32_t*>(staging)[i];
+    return staging[i];
 }
 
 __device__ __forceinline__ uint32_t region_of(int32_t key, const TableView& t) {
@@ -130,6 +145,7 @@ __global__ void __launch_bounds__(kScanBlock) k_region_scan(const uint32_t* __re
     if (threadIdx.x == kScanBlock - 1) start[regions] = part[kScanBlock - 1];
 }
 
+template <bool KO>
 __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __restrict__ jobs, RegionJob job0,
                                                             const BatchItem* __restrict__ items, uint32_t nitems,
                                                             uint64_t n, uint64_t rpi, uint32_t* __restrict__ cursor,
@@ -175,7 +191,7 @@ __global__ void __launch_bounds__(kRBlock) k_region_scatter(const RegionJob* __r
                     continue;
                 }
                 const uint32_t pos = atomicAdd(sh + region_of(key[u], sj.t), 1u);
-                staging[pos] = ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u];
+                stage_put<KO>(staging, pos, ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u]);
             }
         }
     }
@@ -200,6 +216,7 @@ struct WarpSort {
 // global cursor reservation per region -- and stores runs of consecutive
 // staging rows, with no block-wide barrier.  A tile whose regions span more
 // than kWarpSpan takes one cursor increment per row instead.
+template <bool KO>
 __global__ void __launch_bounds__(kRBlock, 2) k_region_scatter_sorted(RegionJob job, uint64_t n,
                                                                     uint32_t* __restrict__ cursor,
                                                                     unsigned long long* __restrict__ staging,
@@ -245,7 +262,7 @@ __global__ void __launch_bounds__(kRBlock, 2) k_region_scatter_sorted(RegionJob 
             for (int u = 0; u < kWarpTileRows; ++u)
                 if (in[u]) {
                     const uint32_t pos = atomicAdd(cursor + job.region0 + reg[u], 1u);
-                    staging[pos] = ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u];
+                    stage_put<KO>(staging, pos, ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u]);
                 }
             continue;
         }
@@ -295,7 +312,7 @@ __global__ void __launch_bounds__(kRBlock, 2) k_region_scatter_sorted(RegionJob 
                 ws.reg[p] = (uint8_t)reg[u];
             }
         __syncwarp();
-        for (uint32_t j = lane; j < total; j += 32) staging[ws.base[ws.reg[j]] + j] = ws.val[j];
+        for (uint32_t j = lane; j < total; j += 32) stage_put<KO>(staging, ws.base[ws.reg[j]] + j, ws.val[j]);
         __syncwarp();  // the warp's buffers are free for its next tile
     }
 }
@@ -404,12 +421,13 @@ __device__ __forceinline__ uint32_t next_region(uint32_t g, uint32_t regions, co
 
 // Staging rows [s0, s1) of a region, the first kBuildRows * kRBuildBlock of
 // them, into registers (rows past s1 read as empty).
+template <bool KO>
 __device__ __forceinline__ void load_region_rows(const unsigned long long* staging, uint32_t s0, uint32_t s1,
                                                  unsigned long long (&v)[kBuildRows]) {
 #pragma unroll
     for (int u = 0; u < kBuildRows; ++u) {
         const uint32_t i = s0 + threadIdx.x + u * kRBuildBlock;
-        v[u] = i < s1 ? staging[i] : kEmptySlot;
+        v[u] = i < s1 ? stage_get<KO>(staging, i) : kEmptySlot;
     }
 }
 
@@ -435,7 +453,7 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
     int64_t cur = -1;
     uint32_t g = next_region(blockIdx.x, regions, start, fresh);
     unsigned long long v[kBuildRows];
-    if (g < regions) load_region_rows(staging, start[g], start[g + 1], v);
+    if (g < regions) load_region_rows<KO>(staging, start[g], start[g + 1], v);
     while (g < regions) {
         const uint32_t s0 = start[g], s1 = start[g + 1];
         const uint32_t j = (jobs && njobs > 1) ? job_of_region(jobs, njobs, g) : 0u;
@@ -488,11 +506,11 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
                 else ovf[atomicAdd(ovf_count, 1u)] = ((unsigned long long)j << 32) | i;  // the run leaves the region
             }
             if (i0 + kRBuildBlock * kBuildRows >= s1) break;
-            load_region_rows(staging, i0 + kRBuildBlock * kBuildRows - threadIdx.x, s1, v);  // a large region
+            load_region_rows<KO>(staging, i0 + kRBuildBlock * kBuildRows - threadIdx.x, s1, v);  // a large region
         }
         __syncthreads();
         const uint32_t gn = next_region(g + gridDim.x, regions, start, fresh);
-        if (gn < regions) load_region_rows(staging, start[gn], start[gn + 1], v);  // in flight from here on
+        if (gn < regions) load_region_rows<KO>(staging, start[gn], start[gn + 1], v);  // in flight from here on
         bool dup = false;
         for (uint32_t b = threadIdx.x; b < nb; b += kRBuildBlock) dup |= bucket_has_dup<KO>(tab, fill, nb, b);
         fence_proxy_async_smem();  // the inserts, before the bulk store reads them
@@ -515,6 +533,7 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
 
 // Rows whose run left their region, into the global table (each entry:
 // job << 32 | staging row).
+template <bool KO>
 __global__ void k_region_overflow(const RegionJob* __restrict__ jobs, RegionJob job0,
                                   const unsigned long long* __restrict__ staging,
                                   const unsigned long long* __restrict__ ovf, const uint32_t* ovf_count, uint32_t* err) {
@@ -522,7 +541,7 @@ __global__ void k_region_overflow(const RegionJob* __restrict__ jobs, RegionJob 
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < cnt; x += gridDim.x * blockDim.x) {
         const unsigned long long e = ovf[x];
         const TableView t = jobs ? jobs[e >> 32].t : job0.t;
-        const unsigned long long v = staging[(uint32_t)e];
+        const unsigned long long v = stage_get<KO>(staging, (uint32_t)e);
         bool dup = false, ok = false;
         table_insert(t, (int32_t)(uint32_t)v, (int32_t)(uint32_t)(v >> 32), err, dup, ok);
         if (ok) atomicAdd(t.meta + 2, 1ull);
@@ -566,11 +585,15 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
     const bool sorted = partitioned && !items && njobs == 1;
     const size_t wsmem = sizeof(WarpSort) * (kRBlock / 32);
     const size_t tsmem = (32ull + 4ull) * kRegionBuckets;  // the region, then its fill counters
+    // every job of one launch has the same slot layout (all key-only or none); a
+    // key-only launch stages 4-byte keys
+    const bool ko = job0.t.key_only != 0;
+    const void* kscat = ko ? (const void*)k_region_scatter<true> : (const void*)k_region_scatter<false>;
+    const void* ksort = ko ? (const void*)k_region_scatter_sorted<true> : (const void*)k_region_scatter_sorted<false>;
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_region_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
-        (e = cudaFuncSetAttribute(k_region_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
-        (e = cudaFuncSetAttribute(k_region_scatter_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)wsmem)) ||
+        (e = cudaFuncSetAttribute(kscat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)) ||
+        (e = cudaFuncSetAttribute(ksort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem)) ||
         (e = cudaFuncSetAttribute(k_region_build<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)) ||
         (e = cudaFuncSetAttribute(k_region_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)))
         return e;
@@ -589,22 +612,23 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
     if (sorted && n) {
         const uint64_t tiles = (n + kWarpTile - 1) / kWarpTile;
         const uint64_t ctas = (tiles + kRBlock / 32 - 1) / (kRBlock / 32);
-        const int grid = (int)std::min<uint64_t>(
-            ctas, (uint64_t)occupancy_grid((const void*)k_region_scatter_sorted, kRBlock, wsmem, ctx));
-        k_region_scatter_sorted<<<grid, kRBlock, wsmem, s>>>(job0, n, sc.cursor, sc.staging, ctx->d_err);
+        const int grid = (int)std::min<uint64_t>(ctas, (uint64_t)occupancy_grid(ksort, kRBlock, wsmem, ctx));
+        if (ko) k_region_scatter_sorted<true><<<grid, kRBlock, wsmem, s>>>(job0, n, sc.cursor, sc.staging, ctx->d_err);
+        else k_region_scatter_sorted<false><<<grid, kRBlock, wsmem, s>>>(job0, n, sc.cursor, sc.staging, ctx->d_err);
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     } else if (nitems) {
-        const int grid = (int)std::min<uint64_t>(
-            nitems, (uint64_t)occupancy_grid((const void*)k_region_scatter, kRBlock, hsmem, ctx));
-        k_region_scatter<<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item, sc.cursor,
-                                                      sc.staging, ctx->d_err);
+        const int grid = (int)std::min<uint64_t>(nitems, (uint64_t)occupancy_grid(kscat, kRBlock, hsmem, ctx));
+        if (ko)
+            k_region_scatter<true><<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item,
+                                                                sc.cursor, sc.staging, ctx->d_err);
+        else
+            k_region_scatter<false><<<grid, kRBlock, hsmem, s>>>(d_jobs, job0, items, nitems, n, rows_per_item,
+                                                                 sc.cursor, sc.staging, ctx->d_err);
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     }
     {
-        // every job of one launch has the same slot layout (all key-only or none)
-        const bool ko = job0.t.key_only != 0;
         const void* kb = ko ? (const void*)k_region_build<true> : (const void*)k_region_build<false>;
         const int grid = (int)std::min<uint64_t>(total_regions,
                                                  (uint64_t)occupancy_grid(kb, kRBuildBlock, tsmem, ctx));
@@ -619,7 +643,8 @@ cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0,
         ctx->launches++;
         if ((e = cudaGetLastError())) return e;
     }
-    k_region_overflow<<<sms * 2, 256, 0, s>>>(d_jobs, job0, sc.staging, sc.ovf, sc.ovf_count, ctx->d_err);
+    if (ko) k_region_overflow<true><<<sms * 2, 256, 0, s>>>(d_jobs, job0, sc.staging, sc.ovf, sc.ovf_count, ctx->d_err);
+    else k_region_overflow<false><<<sms * 2, 256, 0, s>>>(d_jobs, job0, sc.staging, sc.ovf, sc.ovf_count, ctx->d_err);
     ctx->launches++;
     return cudaGetLastError();
 }
