@@ -44,8 +44,6 @@ struct mgv_batch {
     unsigned char* group_zero = nullptr;  // sums, counts and specials (zeroed per run)
     size_t group_zero_bytes = 0;
     uint32_t* out_counts = nullptr;
-    mgv_group_row* out_rows = nullptr;
-    uint64_t out_rows_total = 0;
     ChainDev* d_qs = nullptr;
     RegionJob* d_jobs = nullptr;  // one shared-memory build job per query
     RegionScratch rsc{};
@@ -57,8 +55,11 @@ struct mgv_batch {
     BatchItem* d_compact_items = nullptr;
     uint32_t n_build = 0, n_probe = 0, n_compact = 0;
     std::vector<uint64_t> out_offset;  // first packed row of each query
-    // host landing zone
+    // host landing zone: the packing kernel writes each query's rows straight into
+    // it (pinned, mapped), so only the groups found cross to the host, not every
+    // query's max_groups rows
     mgv_group_row* h_rows = nullptr;
+    mgv_group_row* h_rows_dev = nullptr;  // the same memory as the device addresses it
     uint32_t* h_counts = nullptr;
     uint32_t* h_err = nullptr;
     // graph
@@ -114,9 +115,6 @@ mgv_status enqueue_run(mgv_batch* b, cudaStream_t s) {
     MGV_CUDA_TRY(launch_batch(b->d_qs, b->d_outs, b->d_probe_items, b->n_probe, b->d_compact_items, b->n_compact,
                               (int)b->cfg.probe_ctas_per_sm, b->cfg.item_order, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(b->h_counts, b->out_counts, sizeof(uint32_t) * b->q.size(), cudaMemcpyDeviceToHost, s));
-    if (b->out_rows_total)
-        MGV_CUDA_TRY(cudaMemcpyAsync(b->h_rows, b->out_rows, sizeof(mgv_group_row) * b->out_rows_total,
-                                     cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaMemcpyAsync(b->h_err, ctx->d_err, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     return MGV_OK;
 }
@@ -206,7 +204,6 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     b->out_offset.resize(nq);
     uint64_t out_total = 0;
     for (uint32_t i = 0; i < nq; ++i) { b->out_offset[i] = out_total; out_total += qs[i].max_groups; }
-    const size_t rows_off = take(sizeof(mgv_group_row) * std::max<uint64_t>(out_total, 1));
     const size_t qs_off = take(sizeof(ChainDev) * std::max(nq, 1u));
     const size_t jobs_off = take(sizeof(RegionJob) * std::max(nq, 1u));
     std::vector<uint32_t> region0(nq);
@@ -252,6 +249,12 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         delete b;
         return cuda_fail(e, "mgv_batch_create");
     }
+    e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&b->h_rows_dev), b->h_rows, 0);
+    if (e != cudaSuccess) {
+        free_batch_device(b);
+        delete b;
+        return cuda_fail(e, "mgv_batch_create: mapped landing zone");
+    }
     b->h_counts = reinterpret_cast<uint32_t*>(b->h_rows + std::max<uint64_t>(out_total, 1));
     b->h_err = b->h_counts + nq;
     unsigned char* A = b->arena;
@@ -263,8 +266,6 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
     b->group_zero = A + gzero_begin;
     b->group_zero_bytes = gzero_end - gzero_begin;
     b->out_counts = reinterpret_cast<uint32_t*>(A + counts_off);
-    b->out_rows = reinterpret_cast<mgv_group_row*>(A + rows_off);
-    b->out_rows_total = out_total;
     b->d_qs = reinterpret_cast<ChainDev*>(A + qs_off);
     b->d_jobs = reinterpret_cast<RegionJob*>(A + jobs_off);
     b->rsc = carve_region_scratch(A + rsc_off, total_regions, build_total);
@@ -320,7 +321,7 @@ mgv_status mgv_batch_create(mgv_ctx* ctx, const mgv_query_desc* qs, uint32_t nq,
         c.smem_groups = std::min(gcap[i], kMaxSmemGroups);
         hj[i] = RegionJob{t, qs[i].build_keys, qs[i].build_payloads, nullptr, 0, region0[i],
                           (nbk[i] + kRegionBuckets - 1) / kRegionBuckets, 0};
-        ho[i] = BatchOut{g, b->out_rows + b->out_offset[i], b->out_counts + i, qs[i].max_groups, 0};
+        ho[i] = BatchOut{g, b->h_rows_dev + b->out_offset[i], b->out_counts + i, qs[i].max_groups, 0};
     }
     e = cudaMemcpy(b->d_qs, hq.data(), sizeof(ChainDev) * nq, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_jobs, hj.data(), sizeof(RegionJob) * nq, cudaMemcpyHostToDevice);
