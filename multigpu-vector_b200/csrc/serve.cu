@@ -315,6 +315,20 @@ void finish(mgv_server* S, Inflight& sl) {
     sl.busy = false;
 }
 
+// A batch that the GPU reported an error for (lock held): its requests fail
+// with MGV_ECUDA, its landing zone and memory charge are released.
+void fail_slot(mgv_server* S, Inflight& sl, cudaError_t e) {
+    (void)cuda_fail(e, "mgv_server: batch");
+    for (auto& q : sl.reqs) {
+        S->used -= q->bytes;
+        complete(S, q, MGV_ECUDA);
+    }
+    if (sl.land) sl.land->attached = false;
+    sl.land = nullptr;
+    sl.reqs.clear();
+    sl.busy = false;
+}
+
 // Plain mode: one request through the operator API (lock not held).
 // The group-by operator of the single-query chain for max_groups.  One per
 // power-of-two class: its table (2 x max_groups, rounded up to a power of two)
@@ -376,12 +390,20 @@ void scheduler(mgv_server* S) {
             S->done_cv.notify_all();
             continue;
         }
-        // 1. harvest finished batches; the host copies run outside the lock
+        // 1. harvest finished batches; the host copies run outside the lock.  A
+        // batch whose stream reports an error (not just "not ready") fails its
+        // requests, so no waiter waits for results that will never come.
         bool any_busy = false;
         for (auto& sl : S->slots) {
-            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) {
-                finish(S, sl);
-                S->done_cv.notify_all();
+            if (sl.busy) {
+                const cudaError_t q = cudaEventQuery(sl.done);
+                if (q == cudaSuccess) {
+                    finish(S, sl);
+                    S->done_cv.notify_all();
+                } else if (q != cudaErrorNotReady) {
+                    fail_slot(S, sl, q);
+                    S->done_cv.notify_all();
+                }
             }
             any_busy |= sl.busy;
         }
