@@ -500,7 +500,9 @@ __global__ void __launch_bounds__(kRBuildBlock, 3) k_region_build(const RegionJo
 #pragma unroll
             for (int u = 0; u < kBuildRows; ++u) {
                 const uint32_t i = i0 + u * kRBuildBlock;
-                if (i >= s1) continue;
+                // past the region, or a gap slot of a partition's range (the
+                // reserved key goes to the side list, never into staging)
+                if (i >= s1 || (int32_t)(uint32_t)v[u] == kEmptyKey) continue;
                 const uint32_t hb = home_bucket((int32_t)(uint32_t)v[u], sj.t) - b0;
                 if (region_insert<KO>(tab, fill, nb, hb, v[u])) ++ins;
                 else ovf[atomicAdd(ovf_count, 1u)] = ((unsigned long long)j << 32) | i;  // the run leaves the region
@@ -549,7 +551,160 @@ __global__ void k_region_overflow(const RegionJob* __restrict__ jobs, RegionJob 
     }
 }
 
+// ---- staging of a partition op's single run ---------------------------------
+//
+// A partition op's single run gives each partition's rows as one range
+// [ends[p-1], ends[p]), and when the table's partition slices are whole
+// regions (bpp a multiple of kRegionBuckets) every region lies in one
+// partition.  One CTA per partition then counts its rows per region in
+// shared memory, and stages them region-major inside the partition's own
+// range -- the regions' starts are the range's start plus a prefix sum, so
+// no global histogram, scan or cursor is needed, and the partition's rows
+// (just written by the partition op) are read from L2 twice.  Rows with the
+// reserved key go to the side list; their slots at the range's end are
+// filled with the reserved key, which the region build skips.
+constexpr int kPartScatterBlock = 1024;
+constexpr int kPartScatterRows = 4;  // loads per thread in flight
+
+template <bool KO>
+__global__ void __launch_bounds__(kPartScatterBlock) k_region_part_scatter(RegionJob job,
+                                                                           const unsigned long long* __restrict__ ends,
+                                                                           uint32_t P, uint32_t rpp,
+                                                                           uint32_t* __restrict__ start,
+                                                                           unsigned long long* __restrict__ staging,
+                                                                           uint32_t* err) {
+    extern __shared__ uint32_t cnt[];  // rpp counters, then rpp cursors
+    uint32_t* cur = cnt + rpp;
+    __shared__ uint32_t side_rows;
+    const uint32_t lane = lane_id();
+    const uint32_t bpp = job.t.bpp;
+    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
+        const uint64_t lo = p ? ends[p - 1] : 0ull, hi = ends[p];
+        __syncthreads();  // the previous partition is done with the counters
+        for (uint32_t r = threadIdx.x; r < rpp; r += kPartScatterBlock) cnt[r] = 0;
+        if (threadIdx.x == 0) side_rows = 0;
+        __syncthreads();
+        // 1. rows per region
+        for (uint64_t i0 = lo + threadIdx.x; i0 < hi; i0 += (uint64_t)kPartScatterBlock * kPartScatterRows) {
+            int32_t key[kPartScatterRows];
+#pragma unroll
+            for (int u = 0; u < kPartScatterRows; ++u) {
+                const uint64_t i = i0 + (uint64_t)u * kPartScatterBlock;
+                key[u] = i < hi ? __ldg(job.keys + i) : kEmptyKey;
+            }
+#pragma unroll
+            for (int u = 0; u < kPartScatterRows; ++u)
+                if (key[u] != kEmptyKey) atomicAdd(cnt + __umulhi(murmur32((uint32_t)key[u]), bpp) / kRegionBuckets, 1u);
+        }
+        __syncthreads();
+        // the regions' starts inside the partition's range
+        if (threadIdx.x < 32) {
+            uint32_t run = 0;
+            for (uint32_t r0 = 0; r0 < rpp; r0 += 32) {
+                const uint32_t r = r0 + lane;
+                const uint32_t c = r < rpp ? cnt[r] : 0u;
+                uint32_t x = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= (uint32_t)o) x += y;
+                }
+                if (r < rpp) {
+                    const uint32_t off = (uint32_t)lo + run + x - c;
+                    cur[r] = off;
+                    start[(uint64_t)p * rpp + r] = off;
+                }
+                run += __shfl_sync(0xffffffffu, x, 31);
+            }
+        }
+        if (p == P - 1 && threadIdx.x == 0) start[(uint64_t)P * rpp] = (uint32_t)hi;
+        __syncthreads();
+        // 2. the rows, region-major; a warp's rows of one region take consecutive slots
+        for (uint64_t i0 = lo + threadIdx.x;; i0 += (uint64_t)kPartScatterBlock * kPartScatterRows) {
+            const uint64_t base = i0 - threadIdx.x;  // uniform across the CTA
+            if (base >= hi) break;
+            int32_t key[kPartScatterRows], pay[kPartScatterRows];
+#pragma unroll
+            for (int u = 0; u < kPartScatterRows; ++u) {
+                const uint64_t i = i0 + (uint64_t)u * kPartScatterBlock;
+                const bool in = i < hi;
+                key[u] = in ? __ldg(job.keys + i) : kEmptyKey;
+                pay[u] = (!KO && in && job.pays) ? __ldg(job.pays + i) : 0;
+                if (in && key[u] == kEmptyKey) {  // the side list (its duplicates are seen from its count)
+                    bool d, ok;
+                    table_insert(job.t, key[u], pay[u], err, d, ok);
+                    atomicAdd(&side_rows, 1u);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kPartScatterRows; ++u) {
+                const bool row = key[u] != kEmptyKey;
+                const uint32_t r = row ? __umulhi(murmur32((uint32_t)key[u]), bpp) / kRegionBuckets : 0xffffffffu;
+                const uint32_t peers = __match_any_sync(0xffffffffu, r);
+                const uint32_t leader = __ffs(peers) - 1;
+                uint32_t pos = 0;
+                if (row && lane == leader) pos = atomicAdd(cur + r, (uint32_t)__popc(peers));
+                pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(peers & ((1u << lane) - 1u));
+                if (row) stage_put<KO>(staging, pos, ((unsigned long long)(uint32_t)pay[u] << 32) | (uint32_t)key[u]);
+            }
+        }
+        __syncthreads();
+        // the reserved-key rows' slots at the end of the range
+        const uint32_t nside = side_rows;
+        for (uint32_t k = threadIdx.x; k < nside; k += kPartScatterBlock)
+            stage_put<KO>(staging, (uint32_t)(hi - nside) + k, kEmptySlot);
+    }
+}
+
 }  // namespace
+
+bool region_build_partitioned_fits(const TableView& t) {
+    return t.bpp % kRegionBuckets == 0 && t.bpp / kRegionBuckets <= 4096;
+}
+
+cudaError_t launch_build_regions_partitioned(const RegionJob& job, const unsigned long long* ends, uint64_t n,
+                                             const RegionScratch& sc, cudaStream_t s, Context* ctx) {
+    const uint32_t P = job.t.radix_mask + 1;
+    const uint32_t rpp = job.t.bpp / kRegionBuckets;
+    const uint32_t regions = P * rpp;
+    const bool ko = job.t.key_only != 0;
+    const size_t psmem = 8ull * rpp;
+    const size_t tsmem = (32ull + 4ull) * kRegionBuckets;
+    const void* kp = ko ? (const void*)k_region_part_scatter<true> : (const void*)k_region_part_scatter<false>;
+    const void* kb = ko ? (const void*)k_region_build<true> : (const void*)k_region_build<false>;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem)) ||
+        (e = cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)))
+        return e;
+    if ((e = cudaMemsetAsync(sc.ovf_count, 0, 4, s))) return e;
+    if (n) {
+        const int grid = (int)std::min<uint64_t>(P, (uint64_t)occupancy_grid(kp, kPartScatterBlock, psmem, ctx));
+        if (ko)
+            k_region_part_scatter<true><<<grid, kPartScatterBlock, psmem, s>>>(job, ends, P, rpp, sc.start, sc.staging,
+                                                                                ctx->d_err);
+        else
+            k_region_part_scatter<false><<<grid, kPartScatterBlock, psmem, s>>>(job, ends, P, rpp, sc.start,
+                                                                                 sc.staging, ctx->d_err);
+        ctx->launches++;
+        if ((e = cudaGetLastError())) return e;
+    } else {  // nothing staged: every region is empty
+        if ((e = cudaMemsetAsync(sc.start, 0, 4ull * (regions + 1), s))) return e;
+    }
+    const int grid = (int)std::min<uint64_t>(regions, (uint64_t)occupancy_grid(kb, kRBuildBlock, tsmem, ctx));
+    if (ko)
+        k_region_build<true><<<grid, kRBuildBlock, tsmem, s>>>(nullptr, job, 1, regions, sc.start, sc.staging, sc.ovf,
+                                                               sc.ovf_count, 1u, ctx->d_err);
+    else
+        k_region_build<false><<<grid, kRBuildBlock, tsmem, s>>>(nullptr, job, 1, regions, sc.start, sc.staging,
+                                                                sc.ovf, sc.ovf_count, 1u, ctx->d_err);
+    ctx->launches++;
+    if ((e = cudaGetLastError())) return e;
+    const int sms = ctx->prop.multiProcessorCount;
+    if (ko) k_region_overflow<true><<<sms * 2, 256, 0, s>>>(nullptr, job, sc.staging, sc.ovf, sc.ovf_count, ctx->d_err);
+    else k_region_overflow<false><<<sms * 2, 256, 0, s>>>(nullptr, job, sc.staging, sc.ovf, sc.ovf_count, ctx->d_err);
+    ctx->launches++;
+    return cudaGetLastError();
+}
 
 size_t region_scratch_bytes(uint32_t regions, uint64_t rows) {
     auto a = [](size_t x) { return (x + 255) & ~(size_t)255; };

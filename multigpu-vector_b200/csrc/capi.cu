@@ -720,6 +720,7 @@ static mgv_status op_reset(Op* o, cudaStream_t s) {
             break;
         case OpKind::Partition:
             o->pt_fill = 0;
+            o->pt_runs = 0;
             o->pt_offered = 0;
             o->pt_filtered = false;
             o->pt_hist_valid = true;
@@ -861,10 +862,13 @@ mgv_status mgv_op_close(mgv_op* o, void* stream) {
             hb->hb_partitioned = hb->kind == OpKind::HashBuild && hb->hb.key_col == o->pt.key_col &&
                                  hb->table.radix_mask == (1u << o->pt.radix_bits) - 1u &&
                                  hb->table.radix_shift == o->pt.radix_shift;
+            // one run: the partition ends left by its scatter locate each partition's rows
+            hb->hb_part_ends = hb->hb_partitioned && o->pt_runs == 1 ? o->pt_dev : nullptr;
             const int32_t* cols[MGV_MAX_COLS];
             for (uint32_t c = 0; c < o->pt_ncols; ++c) cols[c] = o->pt_store + c * o->pt.max_rows;
             st = consume_cols(o->parent, cols, o->pt_ncols, o->pt_fill, s);
             hb->hb_partitioned = false;
+            hb->hb_part_ends = nullptr;
         }
     }
     mgv_status st2 = mgv_op_close(static_cast<mgv_op*>(o->parent), stream);  // after_close
@@ -1010,6 +1014,7 @@ static mgv_status consume_partition(Op* part, Op* sel, const int32_t* const* col
     if (ncols != part->pt_ncols) return fail(MGV_EINVAL, "partition: every consume must carry the same columns");
     if (n == 0) return MGV_OK;
     part->pt_offered += n;
+    part->pt_runs++;
     if (sel) part->pt_filtered = true;
     MGV_CUDA_TRY(cudaMemsetAsync(part->pt_dev, 0, sizeof(unsigned long long) * P, s));
     MGV_CUDA_TRY(launch_partition_hist(cols, n, sel != nullptr, sel ? sel->sel.col : 0, sel ? sel->sel.bound : 0,
@@ -1140,6 +1145,12 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
                 term->rb_bytes = need;
             }
             const RegionJob job{term->table, cols[kc], pays, filt, bound, 0, regions, 0};
+            if (fresh && term->hb_part_ends && !sel && region_build_partitioned_fits(term->table)) {
+                MGV_CUDA_TRY(launch_build_regions_partitioned(job, term->hb_part_ends, n,
+                                                              carve_region_scratch(term->rb_scratch, regions, n), s,
+                                                              ctx));
+                return MGV_OK;
+            }
             // items: two per SM, each worth zeroing and flushing its region histogram
             const uint64_t rows_per_item =
                 std::max<uint64_t>({8ull * regions, 4096, n / (2ull * ctx->prop.multiProcessorCount) + 1});

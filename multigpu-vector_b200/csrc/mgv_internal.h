@@ -174,6 +174,7 @@ struct Op {
     uint32_t pt_ncols = 0;
     uint64_t pt_fill = 0;                 // rows stored (read back at close)
     uint64_t pt_offered = 0;              // rows consumed since open (host count)
+    uint32_t pt_runs = 0;                 // consumes with rows since open (each stores one partition-major run)
     bool pt_filtered = false;             // a select fed a consume: only the device knows pt_fill
     bool pt_hist_valid = true;            // pt_hist read back (else read at mgv_op_result)
     cudaStream_t pt_close_stream = nullptr;
@@ -182,6 +183,7 @@ struct Op {
     std::vector<uint64_t> pt_hist;        // rows per partition (read back at close)
     bool hb_fresh = false;  // opened, nothing consumed yet: the table is not cleared yet
     bool hb_partitioned = false;  // the rows being consumed are a partition op's run on the table's radix bits
+    const unsigned long long* hb_part_ends = nullptr;  // that run's partition ends (device), when it is the only run
     // host ingest (mgv_op_consume_host): the copy stream and, per buffer in
     // flight, events for "slice copied" and "slice consumed"
     cudaStream_t in_stream = nullptr;
@@ -310,6 +312,13 @@ RegionScratch carve_region_scratch(void* base, uint32_t regions, uint64_t rows);
 // and are not cleared beforehand; every region is written.  partitioned
 // (one job, no items): the rows arrive partitioned on the table's radix bits,
 // and are scattered by warps that sort their tiles by region.
+// A fresh radix-laid-out table built from a partition op's single run on its
+// radix bits (ends[p] = one past partition p's last row): per-partition
+// staging in the partition's own range, then the region build.  Only when
+// every partition slice is whole regions (region_build_partitioned_fits).
+bool region_build_partitioned_fits(const TableView& t);
+cudaError_t launch_build_regions_partitioned(const RegionJob& job, const unsigned long long* ends, uint64_t n,
+                                             const RegionScratch& sc, cudaStream_t s, Context* ctx);
 cudaError_t launch_build_regions(const RegionJob* d_jobs, const RegionJob& job0, uint32_t njobs,
                                  const struct BatchItem* items, uint32_t nitems, uint64_t n, uint64_t rows_per_item,
                                  uint32_t total_regions, uint32_t max_job_regions, const RegionScratch& sc,
