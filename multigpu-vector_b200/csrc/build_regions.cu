@@ -564,7 +564,7 @@ __global__ void k_region_overflow(const RegionJob* __restrict__ jobs, RegionJob 
 // reserved key go to the side list; their slots at the range's end are
 // filled with the reserved key, which the region build skips.
 constexpr int kPartScatterBlock = 1024;
-constexpr int kPartScatterRows = 4;  // loads per thread in flight
+constexpr int kPartScatterRows = 8;  // loads per thread in flight
 
 template <bool KO>
 __global__ void __launch_bounds__(kPartScatterBlock) k_region_part_scatter(RegionJob job,
