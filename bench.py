@@ -58,6 +58,43 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measure_build(torch, bhead, bk, bp, nb, stream, args):
+    """The build side on its own: open -> consume(all build rows) -> close of the
+    hash_build operator, rebuilt from scratch each time, L2 flushed before each
+    build by reading 1 GiB; device time with events on the launching stream.
+    Algorithmic bytes: 8 B read (key + payload) + 8 B table write per build tuple."""
+    with torch.cuda.stream(stream):
+        flush = torch.ones(1 << 27, dtype=torch.int64, device="cuda")
+        flush_out = torch.empty((), dtype=torch.int64, device="cuda")
+    reps = max(10, min(args.steps, 50))
+    times = []
+    for i in range(3 + reps):
+        with torch.cuda.stream(stream):
+            torch.sum(flush, dim=0, out=flush_out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bhead.open(stream)
+        bhead.consume_columns([bk, bp], nb, stream)
+        bhead.close(stream)
+        e1.record(stream)
+        stream.synchronize()
+        if i >= 3:
+            times.append(e0.elapsed_time(e1) / 1000.0)
+    del flush, flush_out
+    t = statistics.median(times)
+    peak, kind = measured_peaks()
+    achieved = 16 * nb / t / 1e9
+    return {"value": nb / t, "unit": "build tuples/s", "ms": 1000 * t,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": kind, "algorithmic_bytes_per_build": 16 * nb},
+            "workload": f"hash_build of {nb} unique keys + payloads (open -> consume -> close, region build), "
+                        f"median of {reps}, L2 flushed before each build by reading 1 GiB",
+            "note": "8 B read + 8 B table write per build tuple; the table's empty slots are written too, and "
+                    "the rows are staged by table region once (read and written) before the regions are built",
+            "checked": "the probe steps after it run against the table built last and are checked against the "
+                       "oracle"}
+
+
 def probe_traffic_per_launch():
     """DRAM bytes per probe launch from the committed ncu summary, if any."""
     p = os.path.join(HERE, "profiles", "join_probe_traffic.json")
@@ -276,6 +313,12 @@ def main():
     ap.add_argument("--served-plain-first", action="store_true",
                     help="served: run the plain server before the batched one at each rate")
     ap.add_argument("--saturate", type=int, default=5000, help="served: requests in the closing burst")
+    ap.add_argument("--served-mix", default="sizes", choices=["sizes", "config3"],
+                    help="served: the batched mix's sizes over 16 tables, or config-3 queries over one table")
+    ap.add_argument("--serve-seconds-config3", type=float, default=0.5,
+                    help="served config-3 mix: arrival window per rate")
+    ap.add_argument("--saturate-config3", type=int, default=1000,
+                    help="served config-3 mix: requests in the closing burst")
     ap.add_argument("--gather-ceiling", action="store_true",
                     help="measure the random bucket-read ceilings (line widths 32/64/128 B, LSU and TMA gather4, "
                          "40 and 80 MiB tables) instead of the join")
@@ -332,6 +375,9 @@ def main():
     tb1.record(stream)
     stream.synchronize()
     build_ms = tb0.elapsed_time(tb1)
+    build = None
+    if not args.no_extras:
+        build = measure_build(torch, bhead, bk, bp, nb, stream, args)
     info = hb.result()
 
     def step():
@@ -404,6 +450,8 @@ def main():
     extras = {}
     if world == 1 and not args.no_extras:
         extras = run_extras(args, mgv, torch, ctx)
+    if build is not None:
+        extras["build"] = build
     return finish(args, ctx, info, build_ms, elapsed, kernel_s, launches, clk, cnt, s, e2e, cpu, world, rank,
                   dist, (probe, agg, bhead, hb), nb, npb, tuning, extras, checked, ceiling)
 
@@ -417,6 +465,8 @@ def run_extras(args, mgv, torch, ctx):
         def mark(self, *a):
             pass
 
+    if os.path.join(HERE, "oracle") not in sys.path:
+        sys.path.insert(0, os.path.join(HERE, "oracle"))  # the workloads check their results against the oracle
     sub = argparse.Namespace(**vars(args))
     sub.steps, sub.warmup, sub.batch_config = 5, 3, None
     t0 = time.time()
@@ -427,6 +477,8 @@ def run_extras(args, mgv, torch, ctx):
     torch.cuda.empty_cache()
     batched = workloads.run_batched(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     served = workloads.run_served(sub, mgv, torch, ctx, None, NoClock(), emit=False)
+    torch.cuda.empty_cache()
+    served3 = workloads.run_served(sub, mgv, torch, ctx, None, NoClock(), emit=False, mix="config3")
     torch.cuda.empty_cache()
     delivery = workloads.run_delivery(sub, mgv, torch, ctx, None, NoClock(), emit=False)
     torch.cuda.empty_cache()
@@ -447,10 +499,22 @@ def run_extras(args, mgv, torch, ctx):
                                            "plain": [at[r]["plain"]["p50_ms"], at[r]["plain"]["p99_ms"]]}
                                   for r in at},
                    "workload": served["workload"], "checked": served["checked"]},
+        "served_config3": served_summary(served3),
         "delivery": {"value": delivery["value"], "unit": "rows/s", "host_gbs": delivery["host_gbs"],
                      "workload": delivery["workload"]},
         "extras_wall_s": time.time() - t0,
     }
+
+
+def served_summary(served):
+    """The served figures of one mix for the join line."""
+    at = {r["rate"]: r for r in served["rates"]}
+    pick = ("throughput_qps", "p50_ms", "p99_ms", "mean_ms", "mean_batch", "shared_scans")
+    return {"saturated_qps": served["value"], "saturated_plain_qps": served["saturated"]["plain"]["throughput_qps"],
+            "saturated_speedup_vs_plain": served["saturated_speedup_vs_plain"],
+            "rates": {str(r): {"batched": {k: at[r]["batched"][k] for k in pick},
+                               "plain": {k: at[r]["plain"][k] for k in pick}} for r in at},
+            "workload": served["workload"], "checked": served["checked"]}
 
 
 def run_e2e(mgv, torch, ctx, probe, agg, pk, pp, npb, stream, args, dist, world, want):

@@ -95,7 +95,11 @@ typedef struct mgv_tuning {
                                        power of 2 in [64, 8192]; default 8192        */
     uint32_t select_ctas_per_sm;    /* select -> aggregate kernel: CTAs of 256 threads
                                        per SM, 1..8 (0 = the default, 2)             */
-    uint32_t reserved;
+    uint32_t select_compact;        /* select -> aggregate: 0 = masked fold of every row
+                                       (the default), 1 = warp-ballot compaction of the
+                                       qualifying rows into 128-row vectors that the
+                                       aggregate reads (unstable_select::consume_warp,
+                                       src/operators/select3.cu:19-85); same results */
 } mgv_tuning;
 
 mgv_status mgv_ctx_set_tuning(mgv_ctx *ctx, const mgv_tuning *t);
@@ -469,7 +473,12 @@ typedef struct mgv_server_config {
                               * the operator chain (lower latency); batches
                               * form once a longer queue builds up;
                               * 1: every request is batched                   */
-    uint32_t reserved;
+    uint32_t separate_scans; /* 0: requests of one batch over the same table,
+                              * probe columns and row count that differ only in
+                              * their filter bound share one scan (the columns
+                              * read and the table probed once, each matched row
+                              * aggregated once per filter range); 1: every
+                              * request scans alone                          */
 } mgv_server_config;
 
 typedef struct mgv_server_request {
@@ -487,6 +496,8 @@ typedef struct mgv_server_stats {
     double mean_batch;
     uint64_t resident_table_bytes, peak_bytes;
     uint64_t solo;           /* requests answered alone by the operator chain */
+    uint64_t shared_scans;   /* shared scans launched                         */
+    uint64_t scan_queries;   /* requests answered by shared scans             */
 } mgv_server_stats;
 
 typedef struct mgv_server mgv_server;

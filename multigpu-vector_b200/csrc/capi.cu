@@ -264,6 +264,7 @@ mgv_status mgv_ctx_set_tuning(mgv_ctx* ctx, const mgv_tuning* t) {
     if (gs != 0 && (gs < 64 || gs > kMaxSmemGroups || (gs & (gs - 1)) != 0))
         return fail(MGV_EINVAL, "groupby_smem_slots must be 0 or a power of two in [64, 8192]");
     if (t->select_ctas_per_sm > 8) return fail(MGV_EINVAL, "select_ctas_per_sm must be 0..8");
+    if (t->select_compact > 1) return fail(MGV_EINVAL, "select_compact must be 0 or 1");
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuning = *t;
     return MGV_OK;
@@ -1062,7 +1063,9 @@ static mgv_status consume_cols(Op* head, const int32_t* const* cols, uint32_t nc
             const int32_t ca = term->agg.sum_col_a, cb = term->agg.sum_col_b;
             if (!ref_ok(ca) || !ref_ok(cb)) return fail(MGV_EINVAL, "aggregate column not in input");
             if (n == 0) return MGV_OK;
-            if (!probe) {
+            // select -> aggregate: the masked fold, unless the context asks
+            // for the warp-ballot compaction of the chain kernel
+            if (!probe && !(sel && ctx->tuning.select_compact)) {
                 MGV_CUDA_TRY(launch_select_agg(sel ? cols[sel->sel.col] : nullptr, sel ? sel->sel.bound : 0,
                                                sel != nullptr, ca >= 0 ? cols[ca] : nullptr,
                                                cb >= 0 ? cols[cb] : nullptr, n, term->d_acc, s, ctx));

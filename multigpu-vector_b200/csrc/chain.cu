@@ -272,6 +272,108 @@ __device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const Gr
     }
 }
 
+// ---- shared scans: per-(range, group) cells ------------------------------------
+//
+// A CTA's shared cell table, keyed by (range << 32) | group in 64 bits
+// (EMPTY = ~0, which no range below 2^31 produces); count and the biased
+// two-word sum as in SmemGroups.  Cells that find no shared slot go to the
+// range's global table, which shares its key array (the group directory)
+// with every other range (CellsView).
+
+constexpr uint32_t kCellSlots = 4096;  // shared cells per CTA (80 KiB)
+constexpr unsigned long long kEmptyCell = ~0ull;
+
+struct SmemCells {
+    unsigned long long* keys;
+    uint32_t* cnt;
+    uint32_t* lo;
+    uint32_t* hi;
+    uint32_t* used;
+    uint32_t cap;  // power of two
+};
+
+__host__ __device__ __forceinline__ size_t smem_cells_bytes(uint32_t cap) { return (size_t)cap * 20 + 16; }
+
+__device__ __forceinline__ SmemCells smem_cells_at(unsigned char* base, uint32_t cap) {
+    SmemCells c;
+    c.keys = reinterpret_cast<unsigned long long*>(base);
+    c.cnt = reinterpret_cast<uint32_t*>(base + (size_t)cap * 8);
+    c.lo = c.cnt + cap;
+    c.hi = c.lo + cap;
+    c.used = c.hi + cap;
+    c.cap = cap;
+    return c;
+}
+
+__device__ __forceinline__ uint32_t cell_hash(unsigned long long key, uint32_t cap) {
+    return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (33 + __clz(cap)));  // cap = 2^k: shift = 64 - k
+}
+
+// Range of a filter value that passed the select (f <= b[m-1]): the first j
+// with b[j] >= f.
+__device__ __forceinline__ uint32_t cell_range(const int32_t* b, uint32_t m, int32_t f) {
+    uint32_t lo = 0, hi = m - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (b[mid] >= f) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// One matched row (g, v) of range j, per lane.
+__device__ __forceinline__ void cells_add_row(const SmemCells& sc, const CellsView& cv, uint32_t j, int32_t g,
+                                              int32_t v, uint32_t* err) {
+    const unsigned long long key = ((unsigned long long)j << 32) | (uint32_t)g;
+    uint32_t slot = cell_hash(key, sc.cap);
+#pragma unroll 1
+    for (uint32_t i = 0; i < kGroupProbes; ++i) {
+        unsigned long long k = *((volatile unsigned long long*)(sc.keys + slot));
+        if (k == kEmptyCell) {
+            if (*(volatile uint32_t*)sc.used >= smem_groups_limit(sc.cap)) break;  // stays global
+            k = atomicCAS(sc.keys + slot, kEmptyCell, key);
+            if (k == kEmptyCell) atomicAdd(sc.used, 1u);
+        }
+        if (k == kEmptyCell || k == key) {
+            const uint32_t x = (uint32_t)v ^ 0x80000000u;  // v + 2^31
+            atomicAdd(sc.cnt + slot, 1u);
+            const uint32_t old = atomicAdd(sc.lo + slot, x);
+            if (old + x < old) atomicAdd(sc.hi + slot, 1u);
+            return;
+        }
+        slot = (slot + 1) & (sc.cap - 1);
+    }
+    global_group_add(cells_range(cv, j), g, (unsigned long long)(long long)v, 1ull, err);
+}
+
+__device__ __forceinline__ void smem_cells_init(const SmemCells& sc) {
+    for (uint32_t i = threadIdx.x; i < sc.cap; i += blockDim.x) {
+        sc.keys[i] = kEmptyCell;
+        sc.cnt[i] = 0;
+        sc.lo[i] = 0;
+        sc.hi[i] = 0;
+    }
+    if (threadIdx.x == 0) *sc.used = 0;
+}
+
+__device__ __forceinline__ void smem_cells_flush(const SmemCells& sc, const CellsView& cv, uint32_t* err) {
+    for (uint32_t i = threadIdx.x; i < sc.cap; i += blockDim.x) {
+        const uint32_t c = sc.cnt[i];
+        if (c == 0) continue;
+        const unsigned long long key = sc.keys[i];
+        const unsigned long long biased = ((unsigned long long)sc.hi[i] << 32) | sc.lo[i];
+        global_group_add(cells_range(cv, (uint32_t)(key >> 32)), (int32_t)(uint32_t)key,
+                         biased - ((unsigned long long)c << 31), (unsigned long long)c, err);
+    }
+}
+
+// What a shared scan's chain needs besides the descriptor: the CTA's cell
+// table and the bounds, copied to shared memory.
+struct CellCtx {
+    SmemCells sc;
+    const int32_t* bounds;
+};
+
 // ---- the chain: per-warp processing of a row range ------------------------------
 
 // Value of carried slot `slot` (a run-time index) from the registers of a
@@ -299,7 +401,8 @@ template <bool SEL, bool PROBE, int TERM, bool FIXED = false>
 __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, uint64_t row_lo, uint64_t row_hi,
                                               uint64_t win_first, uint64_t win_stride, uint32_t* ids,
                                               const SmemGroups& sg, unsigned long long& acnt,
-                                              unsigned long long& asum, uint32_t* err) {
+                                              unsigned long long& asum, uint32_t* err,
+                                              const CellCtx* cc = nullptr) {
     constexpr int NS = TERM == kTermSink ? MGV_MAX_COLS : kMaxTermSlots;
     // A batch query's carried slots are fixed (FIXED): key, group, value from
     // input columns 0, 2, 3, so every slot pick below resolves at compile time.
@@ -316,12 +419,18 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
     auto push_vector = [&](uint32_t start, uint32_t cnt) {
         __syncwarp();
         uint32_t rid[4];
+        uint32_t rng[4];  // shared scan: each row's filter range
         bool in[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const uint32_t idx = j * 32 + lane;
             in[j] = idx < cnt;
             rid[j] = ids[(start + idx) & (kIdRing - 1)];
+            rng[j] = 0;
+            if (TERM == kTermCells) {
+                rng[j] = rid[j] >> kCellRowBits;
+                rid[j] &= (1u << kCellRowBits) - 1u;
+            }
         }
         int32_t v[NS][4];
 #pragma unroll
@@ -351,6 +460,8 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
                     const int32_t x = ref1 >= 0 ? val(ref1, j, bp) : 0;
                     group_add_row(sg, a.gt, g, x, err);
                 }
+            } else if (TERM == kTermCells) {
+                if (active) cells_add_row(cc->sc, a.cells, rng[j], val(ref0, j, bp), val(ref1, j, bp), err);
             } else {
                 sink_emit_warp(
                     a.sink, active ? 1u : 0u, [&](uint32_t, uint32_t col) { return val(a.ref[col], j, bp); }, err);
@@ -460,7 +571,11 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
             const uint32_t row = r0 + k * 32 + lane;
             const bool pass = row < len && (!SEL || f[k] <= a.sel_bound);
             const unsigned m = __ballot_sync(0xffffffffu, pass);
-            if (pass) ids[(head + fill + __popc(m & lt)) & (kIdRing - 1)] = row;
+            if (pass) {
+                uint32_t e = row;
+                if (TERM == kTermCells) e |= cell_range(cc->bounds, a.cells.m, f[k]) << kCellRowBits;
+                ids[(head + fill + __popc(m & lt)) & (kIdRing - 1)] = e;
+            }
             fill += __popc(m);
         }
         while (fill >= 128) {
@@ -555,6 +670,90 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_probe(const ChainDev* 
         __syncthreads();
         smem_groups_flush(sg, sq.gt, err);
     }
+}
+
+// Probe phase of shared scans: the items of every scan dealt round-robin, as
+// in k_batch_probe; a scan's matched rows go to their (range, group) cells
+// in the CTA's shared cell table, flushed to the scan's global cells when
+// the CTA moves to another scan.  The scan's bounds sit in shared memory for
+// the range search of every qualifying row.
+__global__ void __launch_bounds__(kChainBlock, 1) k_batch_cells(const ChainDev* __restrict__ qs,
+                                                                const BatchItem* __restrict__ items,
+                                                                uint32_t nitems, uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ChainDev sq;
+    const uint32_t warp = threadIdx.x / 32;
+    uint32_t* rings = reinterpret_cast<uint32_t*>(smem_raw);
+    const SmemGroups no_sg{nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+    CellCtx cc;
+    cc.sc = smem_cells_at(smem_raw + kRingBytes, kCellSlots);
+    int32_t* sb = reinterpret_cast<int32_t*>(smem_raw + kRingBytes + smem_cells_bytes(kCellSlots));
+    cc.bounds = sb;
+
+    int64_t cur = -1;
+    unsigned long long acnt = 0, asum = 0;
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const BatchItem item = items[it];
+        if ((int64_t)item.q != cur) {
+            __syncthreads();  // every warp is done with the previous scan
+            if (cur >= 0) {
+                smem_cells_flush(cc.sc, sq.cells, err);
+                __syncthreads();  // the flush is done reading sq and the cell table
+            }
+            cur = item.q;
+            for (uint32_t i = threadIdx.x; i < sizeof(ChainDev) / 4; i += kChainBlock)
+                reinterpret_cast<uint32_t*>(&sq)[i] = reinterpret_cast<const uint32_t*>(qs + cur)[i];
+            const CellsView cv = qs[cur].cells;
+            for (uint32_t i = threadIdx.x; i < cv.m; i += kChainBlock) sb[i] = cv.bounds[i];
+            smem_cells_init(cc.sc);
+            __syncthreads();
+        }
+        const ChainDev& a = sq;
+        const bool unique = a.table.meta[3] == 0;
+        chain_windows<true, true, kTermCells, true>(a, unique, item.lo, item.hi, warp, kChainWarps,
+                                                    rings + (size_t)warp * kIdRing, no_sg, acnt, asum, err, &cc);
+    }
+    if (cur >= 0) {
+        __syncthreads();
+        smem_cells_flush(cc.sc, sq.cells, err);
+    }
+}
+
+// Turns a scan's per-range cells into per-bound results: block j becomes the
+// sum of blocks 0..j, word by word (sums, counts and the INT32_MIN group's
+// pair alike; the directory is shared, so a group has one slot in every block).
+__global__ void k_cells_prefix(unsigned long long* __restrict__ vals, uint64_t words, uint32_t m) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < words; x += stride) {
+        unsigned long long run = 0;
+        for (uint32_t j = 0; j < m; ++j) {
+            unsigned long long* p = vals + (size_t)j * words + x;
+            run += *p;
+            *p = run;
+        }
+    }
+}
+
+cudaError_t launch_cells(const ChainDev* d_scans, const BatchItem* items, uint32_t nitems, cudaStream_t s,
+                         Context* ctx) {
+    if (nitems == 0) return cudaSuccess;
+    const size_t smem = kRingBytes + smem_cells_bytes(kCellSlots) + sizeof(int32_t) * kMaxCellRanges;
+    cudaError_t e = cudaFuncSetAttribute(k_batch_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (int)std::min<uint64_t>((uint64_t)ctx->prop.multiProcessorCount, nitems);
+    k_batch_cells<<<grid, kChainBlock, smem, s>>>(d_scans, items, nitems, ctx->d_err);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cells_prefix(const CellsView& c, cudaStream_t s, Context* ctx) {
+    if (c.m < 2) return cudaSuccess;
+    const uint64_t words = cell_block_words(c.cap);
+    const uint64_t want = (words + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->prop.multiProcessorCount * 8;
+    k_cells_prefix<<<(int)(want < cap ? want : cap), 256, 0, s>>>(c.vals, words, c.m);
+    ctx->launches++;
+    return cudaGetLastError();
 }
 
 // Packs each query's groups into its output region (unsorted) and counts them;

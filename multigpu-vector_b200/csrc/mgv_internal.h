@@ -220,7 +220,41 @@ cudaError_t launch_probe_agg(const int32_t* keys, const int32_t* pays, uint64_t 
                              const TableView& t, bool unique, uint32_t sum_mode,
                              unsigned long long* acc, cudaStream_t s, Context* ctx);
 // Generic fused chain (chain.cu): [select] -> [probe] -> terminal.
-enum TermKind : int { kTermAgg = 0, kTermGroupby = 1, kTermSink = 2 };
+enum TermKind : int { kTermAgg = 0, kTermGroupby = 1, kTermSink = 2, kTermCells = 3 };
+
+// A shared scan: several select -> join -> group-by requests over the same
+// probe columns and join table that differ only in their filter bound read
+// the columns and probe the table once.  The m distinct bounds, ascending,
+// cut the filter values into m ranges (range j: b[j-1] < f <= b[j]); a
+// matched row adds its (group, value) to one cell (range of its filter,
+// group) only, whatever the number of requests.  A request with bound b[j]
+// is then the sum of ranges 0..j, which one prefix pass over the ranges
+// computes for every request at once.
+//
+// Cells live in m group tables that share one key array (the group
+// directory, `cap` slots): range j's table is {keys, v + j*(2 cap + 2),
+// +cap, +2 cap} over one block of u64 values, so a group has the same slot
+// in every range and the prefix is a flat sum over the blocks.
+struct CellsView {
+    const int32_t* bounds;       // m ascending distinct filter bounds
+    uint32_t m;
+    uint32_t cap;                // directory slots, power of two
+    int32_t* keys;               // the group directory (EMPTY = INT32_MIN)
+    unsigned long long* vals;    // m blocks of [sums (cap) | counts (cap) | special sum, count]
+};
+constexpr uint32_t kCellRowBits = 20;        // ring entries: row offset (low bits) | range (high bits)
+constexpr uint32_t kMaxCellRanges = 2048;    // distinct bounds per shared scan (range index < 2^11)
+__host__ __device__ __forceinline__ size_t cell_block_words(uint32_t cap) { return 2ull * cap + 2; }
+__host__ __device__ __forceinline__ GroupTableView cells_range(const CellsView& c, uint32_t j) {
+    GroupTableView g;
+    g.keys = c.keys;
+    g.sums = c.vals + (size_t)j * cell_block_words(c.cap);
+    g.counts = g.sums + c.cap;
+    g.special = g.sums + 2ull * c.cap;
+    g.cap = c.cap;
+    g.pad = 0;
+    return g;
+}
 
 struct ChainArgs {
     const int32_t* cols[MGV_MAX_COLS];
@@ -265,6 +299,7 @@ struct ChainDev {
     GroupTableView gt;
     uint32_t smem_groups;  // shared group-table slots: power of two <= kMaxSmemGroups, 0 = none
     SinkView sink;
+    CellsView cells;       // shared scan (kTermCells): the ranges' cells
 };
 
 constexpr int32_t kBP = 100;  // terminal reference to the build payload
@@ -336,6 +371,12 @@ cudaError_t launch_group_pack(const GroupTableView& gt, mgv_group_row* out, uint
 cudaError_t launch_batch(const ChainDev* d_qs, const BatchOut* d_outs, const BatchItem* probe_items, uint32_t n_probe,
                          const BatchItem* compact_items, uint32_t n_compact, int ctas_per_sm, uint32_t item_order,
                          cudaStream_t s, Context* ctx);
+// Shared scans: the persistent probe -> cells kernel over (scan, rows)
+// items (rows per item < 2^kCellRowBits), then the prefix over each scan's
+// ranges (`scans` are host-side copies of the device descriptors' cells).
+cudaError_t launch_cells(const ChainDev* d_scans, const BatchItem* items, uint32_t nitems, cudaStream_t s,
+                         Context* ctx);
+cudaError_t launch_cells_prefix(const CellsView& c, cudaStream_t s, Context* ctx);
 
 // partition.cu
 cudaError_t launch_partition_hist(const int32_t* const* cols, uint64_t n, bool has_sel, uint32_t sel_col,

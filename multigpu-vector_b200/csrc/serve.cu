@@ -29,6 +29,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "device_common.cuh"
@@ -113,6 +114,7 @@ struct mgv_server {
     // stats
     std::vector<double> latencies;
     uint64_t submitted = 0, completed = 0, batches = 0, rejected = 0, batched_queries = 0, solo = 0;
+    std::atomic<uint64_t> shared_scans{0}, scan_queries{0};  // scans launched, requests they answered
     // plain mode: group-by operators (device tables) reused per max_groups
     std::map<uint32_t, mgv_op*> plain_gb;
     std::vector<std::unique_ptr<Landing>> landings;  // pinned result buffers (lock held)
@@ -167,26 +169,96 @@ mgv_status acquire_landing(mgv_server* S, uint64_t rows, uint32_t ncounts, Landi
 
 // Launch one batch of admitted requests on slot `sl` (scheduler thread, lock
 // not held: it reads only the slot and its requests' immutable parameters).
+// Requests that can share one scan: the same resident table, probe columns,
+// row count and group-table size, differing at most in their filter bound.
+struct ScanKey {
+    const void* table;
+    const int32_t *key, *filter, *group, *value;
+    uint64_t rows;
+    uint32_t cap;
+    bool operator<(const ScanKey& o) const {
+        return std::tie(table, key, filter, group, value, rows, cap) <
+               std::tie(o.table, o.key, o.filter, o.group, o.value, o.rows, o.cap);
+    }
+};
+
+// A shared scan of a batch: its requests, its distinct bounds (ascending) and
+// each request's range (the index of its bound).
+struct Scan {
+    std::vector<uint32_t> reqs;
+    std::vector<int32_t> bounds;
+    std::vector<uint32_t> rank;  // per entry of reqs
+    uint32_t cap = 0;
+    size_t dir_off = 0, vals_off = 0, bounds_off = 0;
+};
+
+// Launch one batch of admitted requests on slot `sl` (scheduler thread, lock
+// not held: it reads only the slot and its requests' immutable parameters).
+// Requests that can share a scan (ScanKey) and number at least two run as
+// one shared scan unless the server was made with separate_scans; the rest
+// run as queries of the batch probe kernel.
 mgv_status launch(mgv_server* S, Inflight& sl) {
     Context* ctx = S->ctx;
     const uint32_t nq = (uint32_t)sl.reqs.size();
-    // device layout: [group keys | zeroed: sums counts specials | counts | rows | qs | outs | items]
+    std::vector<uint32_t> caps(nq);
+    for (uint32_t i = 0; i < nq; ++i) caps[i] = group_cap(sl.reqs[i]->r.max_groups);
+    // ---- shared scans --------------------------------------------------------
+    std::vector<Scan> scans;
+    std::vector<int32_t> scan_of(nq, -1);
+    if (!S->cfg.separate_scans) {
+        std::map<ScanKey, std::vector<uint32_t>> by_key;
+        for (uint32_t i = 0; i < nq; ++i) {
+            const mgv_server_request& r = sl.reqs[i]->r;
+            by_key[ScanKey{sl.reqs[i]->table, r.probe_key, r.probe_filter, r.probe_group, r.probe_value,
+                           r.probe_rows, caps[i]}].push_back(i);
+        }
+        for (auto& kv : by_key) {
+            const std::vector<uint32_t>& v = kv.second;
+            for (size_t c0 = 0; c0 < v.size(); c0 += kMaxCellRanges) {  // at most kMaxCellRanges bounds a scan
+                const size_t c1 = std::min(v.size(), c0 + (size_t)kMaxCellRanges);
+                if (c1 - c0 < 2) continue;
+                Scan sc;
+                sc.reqs.assign(v.begin() + c0, v.begin() + c1);
+                sc.cap = kv.first.cap;
+                for (uint32_t i : sc.reqs) sc.bounds.push_back(sl.reqs[i]->r.filter_bound);
+                std::sort(sc.bounds.begin(), sc.bounds.end());
+                sc.bounds.erase(std::unique(sc.bounds.begin(), sc.bounds.end()), sc.bounds.end());
+                for (uint32_t i : sc.reqs)
+                    sc.rank.push_back((uint32_t)(std::lower_bound(sc.bounds.begin(), sc.bounds.end(),
+                                                                  sl.reqs[i]->r.filter_bound) -
+                                                 sc.bounds.begin()));
+                for (uint32_t i : sc.reqs) scan_of[i] = (int32_t)scans.size();
+                scans.push_back(std::move(sc));
+            }
+        }
+    }
+    // device layout: [group keys, scan directories | zeroed: sums counts specials, scan cells |
+    //                 counts | rows | qs | outs | items | compact items | scans | scan items | bounds]
     size_t off = 0;
     std::vector<size_t> gk(nq), gs(nq), gc(nq), sp(nq);
-    std::vector<uint32_t> caps(nq);
     uint64_t slots = 0, rows = 0;
     for (uint32_t i = 0; i < nq; ++i) {
-        caps[i] = group_cap(sl.reqs[i]->r.max_groups);
+        if (scan_of[i] >= 0) continue;
         gk[i] = off;
         off += 4ull * caps[i];
         slots += caps[i];
     }
+    for (Scan& sc : scans) {
+        sc.dir_off = off;
+        off += 4ull * sc.cap;
+        slots += sc.cap;
+    }
     off = align256(off);
     const size_t zero_begin = off;
     for (uint32_t i = 0; i < nq; ++i) {
+        if (scan_of[i] >= 0) continue;
         gs[i] = off; off += 8ull * caps[i];
         gc[i] = off; off += 8ull * caps[i];
         sp[i] = off; off += 16;
+    }
+    for (Scan& sc : scans) {
+        sc.vals_off = off;
+        off += 8ull * cell_block_words(sc.cap) * sc.bounds.size();
     }
     const size_t zero_end = off;
     off = align256(off);
@@ -196,13 +268,18 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     for (uint32_t i = 0; i < nq; ++i) { sl.offs[i] = rows; rows += sl.reqs[i]->r.max_groups; }
     const size_t rows_off = off;
     off = align256(off + sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1));
-    std::vector<BatchItem> pi, ci;
-    const uint64_t item_rows = 32768;
+    std::vector<BatchItem> pi, ci, si;
+    const uint64_t item_rows = 32768;  // < 2^kCellRowBits, as a shared scan's items must be
     for (uint32_t i = 0; i < nq; ++i) {
-        for (uint64_t lo = 0; lo < sl.reqs[i]->r.probe_rows; lo += item_rows)
-            pi.push_back(BatchItem{i, 0, lo, std::min<uint64_t>(sl.reqs[i]->r.probe_rows, lo + item_rows)});
+        if (scan_of[i] < 0)
+            for (uint64_t lo = 0; lo < sl.reqs[i]->r.probe_rows; lo += item_rows)
+                pi.push_back(BatchItem{i, 0, lo, std::min<uint64_t>(sl.reqs[i]->r.probe_rows, lo + item_rows)});
         for (uint64_t lo = 0; lo <= caps[i]; lo += 65536)
             ci.push_back(BatchItem{i, 0, lo, std::min<uint64_t>((uint64_t)caps[i] + 1, lo + 65536)});
+    }
+    for (uint32_t g = 0; g < (uint32_t)scans.size(); ++g) {
+        const uint64_t n = sl.reqs[scans[g].reqs[0]]->r.probe_rows;
+        for (uint64_t lo = 0; lo < n; lo += item_rows) si.push_back(BatchItem{g, 0, lo, std::min(n, lo + item_rows)});
     }
     const size_t qs_off = off;
     off = align256(off + sizeof(ChainDev) * nq);
@@ -212,6 +289,15 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     off = align256(off + sizeof(BatchItem) * std::max<size_t>(pi.size(), 1));
     const size_t ci_off = off;
     off = align256(off + sizeof(BatchItem) * std::max<size_t>(ci.size(), 1));
+    const size_t scans_off = off;
+    off = align256(off + sizeof(ChainDev) * std::max<size_t>(scans.size(), 1));
+    const size_t si_off = off;
+    off = align256(off + sizeof(BatchItem) * std::max<size_t>(si.size(), 1));
+    for (Scan& sc : scans) {
+        sc.bounds_off = off;
+        off += 4ull * sc.bounds.size();
+    }
+    off = align256(off);
 
     // Each slot keeps its region and only grows it (the slot's previous batch
     // has completed): no allocator runs per batch, so slots never wait on
@@ -228,18 +314,9 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     // a pinned landing zone for the results (rows + counts)
     mgv_status lst = acquire_landing(S, std::max<uint64_t>(rows, 1), nq, sl.land);
     if (lst != MGV_OK) return lst;
-    std::vector<ChainDev> hq(nq);
-    std::vector<BatchOut> ho(nq);
-    for (uint32_t i = 0; i < nq; ++i) {
-        const mgv_server_request& r = sl.reqs[i]->r;
-        GroupTableView g{};
-        g.keys = reinterpret_cast<int32_t*>(A + gk[i]);
-        g.sums = reinterpret_cast<unsigned long long*>(A + gs[i]);
-        g.counts = reinterpret_cast<unsigned long long*>(A + gc[i]);
-        g.special = reinterpret_cast<unsigned long long*>(A + sp[i]);
-        g.cap = caps[i];
-        ChainDev& c = hq[i];
-        c = ChainDev{};
+    // the descriptors of a single request or of a scan (the scan's bound is its largest)
+    auto chain_of = [&](const mgv_server_request& r, const Request& q) {
+        ChainDev c{};
         c.cols[0] = r.probe_key;
         c.cols[1] = r.probe_filter;
         c.cols[2] = r.probe_group;
@@ -253,20 +330,50 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
         c.sel_col = 1;
         c.sel_bound = r.filter_bound;
         c.probe_slot = 0;
-        c.table = sl.reqs[i]->table->table;
+        c.table = q.table->table;
         c.ref[0] = 1;
         c.ref[1] = 2;
         c.nref = 2;
-        c.gt = g;
-        c.smem_groups = std::min(caps[i], kMaxSmemGroups);
+        return c;
+    };
+    std::vector<ChainDev> hq(nq), hs(scans.size());
+    std::vector<BatchOut> ho(nq);
+    for (uint32_t g = 0; g < (uint32_t)scans.size(); ++g) {
+        const Scan& sc = scans[g];
+        const Request& q0 = *sl.reqs[sc.reqs[0]];
+        hs[g] = chain_of(q0.r, q0);
+        hs[g].sel_bound = sc.bounds.back();
+        hs[g].cells = CellsView{reinterpret_cast<const int32_t*>(A + sc.bounds_off), (uint32_t)sc.bounds.size(),
+                                sc.cap, reinterpret_cast<int32_t*>(A + sc.dir_off),
+                                reinterpret_cast<unsigned long long*>(A + sc.vals_off)};
+    }
+    std::vector<uint32_t> rank_of(nq, 0);
+    for (const Scan& sc : scans)
+        for (size_t k = 0; k < sc.reqs.size(); ++k) rank_of[sc.reqs[k]] = sc.rank[k];
+    for (uint32_t i = 0; i < nq; ++i) {
+        const mgv_server_request& r = sl.reqs[i]->r;
+        GroupTableView g{};
+        if (scan_of[i] >= 0) {
+            g = cells_range(hs[scan_of[i]].cells, rank_of[i]);  // the prefix of its ranges
+        } else {
+            g.keys = reinterpret_cast<int32_t*>(A + gk[i]);
+            g.sums = reinterpret_cast<unsigned long long*>(A + gs[i]);
+            g.counts = reinterpret_cast<unsigned long long*>(A + gc[i]);
+            g.special = reinterpret_cast<unsigned long long*>(A + sp[i]);
+            g.cap = caps[i];
+            ChainDev& c = hq[i];
+            c = chain_of(r, *sl.reqs[i]);
+            c.gt = g;
+            c.smem_groups = std::min(caps[i], kMaxSmemGroups);
+        }
         ho[i] = BatchOut{g, reinterpret_cast<mgv_group_row*>(A + rows_off) + sl.offs[i],
                          reinterpret_cast<uint32_t*>(A + counts_off) + i, r.max_groups, 0};
     }
     cudaStream_t s = sl.stream;
-    // The descriptors [qs | outs | probe items | compact items] are laid out
-    // on the device as in the slot's pinned staging area and go over in one
-    // copy.  The staging stays untouched until the slot's batch has
-    // completed (a busy slot is never launched on).
+    // The descriptors [qs | outs | probe items | compact items | scans | scan
+    // items | bounds] are laid out on the device as in the slot's pinned
+    // staging area and go over in one copy.  The staging stays untouched
+    // until the slot's batch has completed (a busy slot is never launched on).
     const size_t desc_bytes = off - qs_off;
     if (desc_bytes > sl.hdesc_cap) {
         if (sl.hdesc) MGV_CUDA_TRY(cudaFreeHost(sl.hdesc));
@@ -280,18 +387,31 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     std::memcpy(sl.hdesc + (outs_off - qs_off), ho.data(), sizeof(BatchOut) * nq);
     if (!pi.empty()) std::memcpy(sl.hdesc + (pi_off - qs_off), pi.data(), sizeof(BatchItem) * pi.size());
     std::memcpy(sl.hdesc + (ci_off - qs_off), ci.data(), sizeof(BatchItem) * ci.size());
+    if (!hs.empty()) std::memcpy(sl.hdesc + (scans_off - qs_off), hs.data(), sizeof(ChainDev) * hs.size());
+    if (!si.empty()) std::memcpy(sl.hdesc + (si_off - qs_off), si.data(), sizeof(BatchItem) * si.size());
+    for (const Scan& sc : scans)
+        std::memcpy(sl.hdesc + (sc.bounds_off - qs_off), sc.bounds.data(), 4 * sc.bounds.size());
     MGV_CUDA_TRY(cudaMemcpyAsync(A + qs_off, sl.hdesc, desc_bytes, cudaMemcpyHostToDevice, s));
     MGV_CUDA_TRY(launch_fill_i32(reinterpret_cast<int32_t*>(A), slots, kEmptyKey, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(A + zero_begin, 0, zero_end - zero_begin, s));
     MGV_CUDA_TRY(cudaMemsetAsync(A + counts_off, 0, 4ull * nq, s));
     MGV_CUDA_TRY(launch_batch(reinterpret_cast<ChainDev*>(A + qs_off), reinterpret_cast<BatchOut*>(A + outs_off),
-                              reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(),
+                              reinterpret_cast<BatchItem*>(A + pi_off), (uint32_t)pi.size(), nullptr, 0u, 0, 0u,
+                              s, ctx));
+    if (!scans.empty()) {
+        MGV_CUDA_TRY(launch_cells(reinterpret_cast<ChainDev*>(A + scans_off), reinterpret_cast<BatchItem*>(A + si_off),
+                                  (uint32_t)si.size(), s, ctx));
+        for (const ChainDev& h : hs) MGV_CUDA_TRY(launch_cells_prefix(h.cells, s, ctx));
+    }
+    MGV_CUDA_TRY(launch_batch(nullptr, reinterpret_cast<BatchOut*>(A + outs_off), nullptr, 0u,
                               reinterpret_cast<BatchItem*>(A + ci_off), (uint32_t)ci.size(), 0, 0u, s, ctx));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.land->counts, A + counts_off, 4ull * nq, cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaMemcpyAsync(sl.land->rows, A + rows_off, sizeof(mgv_group_row) * std::max<uint64_t>(rows, 1),
                                  cudaMemcpyDeviceToHost, s));
     MGV_CUDA_TRY(cudaEventRecord(sl.done, s));
     sl.busy = true;
+    S->shared_scans += scans.size();
+    for (const Scan& sc : scans) S->scan_queries += sc.reqs.size();
     return MGV_OK;
 }
 
@@ -619,6 +739,8 @@ mgv_status mgv_server_stats_get(mgv_server* S, mgv_server_stats* out) {
     out->rejected = S->rejected;
     out->mean_batch = S->batches ? (double)S->batched_queries / S->batches : 0.0;
     out->solo = S->solo;
+    out->shared_scans = S->shared_scans.load();
+    out->scan_queries = S->scan_queries.load();
     out->resident_table_bytes = S->table_bytes;
     out->peak_bytes = S->peak;
     if (!S->latencies.empty()) {
@@ -640,6 +762,8 @@ mgv_status mgv_server_reset_stats(mgv_server* S) {
     std::lock_guard<std::mutex> lk(S->mu);
     S->latencies.clear();
     S->submitted = S->completed = S->batches = S->rejected = S->batched_queries = S->solo = 0;
+    S->shared_scans = 0;
+    S->scan_queries = 0;
     S->peak = S->used + S->table_bytes;
     return MGV_OK;
 }

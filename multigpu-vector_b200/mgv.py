@@ -55,7 +55,7 @@ class CtxInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("probe_kernel", c_uint32), ("probe_rows_per_thread", c_uint32), ("probe_stages", c_uint32),
                 ("probe_ctas_per_sm", c_uint32), ("default_load_factor", c_float),
-                ("groupby_smem_slots", c_uint32), ("select_ctas_per_sm", c_uint32), ("reserved", c_uint32)]
+                ("groupby_smem_slots", c_uint32), ("select_ctas_per_sm", c_uint32), ("select_compact", c_uint32)]
 
 
 class PoolStats(ctypes.Structure):
@@ -130,7 +130,8 @@ class BatchStats(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("memory_budget", c_uint64), ("max_batch", c_uint32), ("max_inflight", c_uint32),
-                ("load_factor", c_float), ("plain", c_uint32), ("batch_solo", c_uint32), ("reserved", c_uint32)]
+                ("load_factor", c_float), ("plain", c_uint32), ("batch_solo", c_uint32),
+                ("separate_scans", c_uint32)]
 
 
 class ServerRequest(ctypes.Structure):
@@ -143,7 +144,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("batches", c_uint64), ("rejected", c_uint64),
                 ("p50_ms", c_double), ("p99_ms", c_double), ("mean_ms", c_double), ("max_ms", c_double),
                 ("mean_batch", c_double), ("resident_table_bytes", c_uint64), ("peak_bytes", c_uint64),
-                ("solo", c_uint64)]
+                ("solo", c_uint64), ("shared_scans", c_uint64), ("scan_queries", c_uint64)]
 
 
 class DiagGatherDesc(ctypes.Structure):
@@ -605,9 +606,11 @@ class Server:
     """mgv_server: continuous batching over resident build tables."""
 
     def __init__(self, ctx: Context, memory_budget: int, max_batch: int = 0, max_inflight: int = 0,
-                 load_factor: float = 0.0, plain: bool = False, batch_solo: bool = False):
+                 load_factor: float = 0.0, plain: bool = False, batch_solo: bool = False,
+                 separate_scans: bool = False):
         h = c_void_p()
-        cfg = ServerConfig(memory_budget, max_batch, max_inflight, load_factor, int(plain), int(batch_solo))
+        cfg = ServerConfig(memory_budget, max_batch, max_inflight, load_factor, int(plain), int(batch_solo),
+                           int(separate_scans))
         _call("mgv_server_create", ctx.h, byref(cfg), byref(h))
         self.h, self.ctx = h, ctx
 

@@ -19,18 +19,26 @@ pytestmark = pytest.mark.gpu
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.json")))
 
 
-def run_select_agg(ctx, cols, n, bound, filter_col=0, sum_col=1):
-    head, agg = mgv.create_sum_select_pipeline(ctx, bound, filter_col, sum_col)
-    head.open()
-    head.consume_columns(cols, n)
-    head.close()
-    r = agg.result()
-    head.destroy()
-    agg.destroy()
+def run_select_agg(ctx, cols, n, bound, filter_col=0, sum_col=1, compact=0):
+    """compact=1 routes the select through the warp-ballot compaction into
+    128-row vectors (mgv_tuning.select_compact) instead of the masked fold."""
+    before = ctx.tuning().select_compact
+    ctx.set_tuning(select_compact=compact)
+    try:
+        head, agg = mgv.create_sum_select_pipeline(ctx, bound, filter_col, sum_col)
+        head.open()
+        head.consume_columns(cols, n)
+        head.close()
+        r = agg.result()
+        head.destroy()
+        agg.destroy()
+    finally:
+        ctx.set_tuning(select_compact=before)
     return r
 
 
-def test_config1_full_size(ctx, torch_cuda):
+@pytest.mark.parametrize("compact", [0, 1], ids=["fold", "ballot"])
+def test_config1_full_size(ctx, torch_cuda, compact):
     """2^22 rows, c0 uniform [0, 2^31), c1 uniform [0, 2^20), c0 < 2^30."""
     torch = torch_cuda
     n = 1 << 22
@@ -38,7 +46,7 @@ def test_config1_full_size(ctx, torch_cuda):
     c1 = torch.empty(n, dtype=torch.int32, device="cuda")
     ctx.gen_uniform(c0, n, 0x5EED0001, 0, 0, 1 << 31)
     ctx.gen_uniform(c1, n, 0x5EED0001, 1, 0, 1 << 20)
-    got = run_select_agg(ctx, [c0, c1], n, (1 << 30) - 1)
+    got = run_select_agg(ctx, [c0, c1], n, (1 << 30) - 1, compact=compact)
     want = po.select_agg(po.gen_uniform(n, 0x5EED0001, 0, 0, 1 << 31), po.gen_uniform(n, 0x5EED0001, 1, 0, 1 << 20),
                          (1 << 30) - 1)
     assert got == want
@@ -46,25 +54,27 @@ def test_config1_full_size(ctx, torch_cuda):
 
 @pytest.mark.parametrize("case", [c for c in GOLDEN["cases"] if c["op"] == "select"],
                          ids=lambda c: f"n{c['input']['n']}_b{c['bound']}")
-def test_golden_sum_select(ctx, torch_cuda, case):
+@pytest.mark.parametrize("compact", [0, 1], ids=["fold", "ballot"])
+def test_golden_sum_select(ctx, torch_cuda, case, compact):
     """COUNT and SUM of the selected column equal sum_select_cpu's answers."""
     s = case["input"]
     a = po.gen_uniform(s["n"], s["seed"], s["stream"], s["lo"], s["range"])
     d = dev(torch_cuda, a if a.size else np.zeros(1, np.int32))
-    cnt, tot = run_select_agg(ctx, [d], s["n"], case["bound"], 0, 0)
+    cnt, tot = run_select_agg(ctx, [d], s["n"], case["bound"], 0, 0, compact=compact)
     assert cnt == case["count"]
     assert i32(tot) == case["sum_int32"]
 
 
 @pytest.mark.parametrize("n", [1, 7, 127, 128, 129, 4095, 4097, 100003])
 @pytest.mark.parametrize("offset", [0, 1])
-def test_ragged_and_unaligned(ctx, torch_cuda, n, offset):
+@pytest.mark.parametrize("compact", [0, 1], ids=["fold", "ballot"])
+def test_ragged_and_unaligned(ctx, torch_cuda, n, offset, compact):
     f = po.gen_uniform(n + 1, 0x5EED0501, 0, -1000, 2000)
     v = po.gen_uniform(n + 1, 0x5EED0501, 1, -(1 << 31), 1 << 32)
     df, dv = dev(torch_cuda, f), dev(torch_cuda, v)
     cols = [df.data_ptr() + 4 * offset, dv.data_ptr() + 4 * offset]
     for bound in (-2000, -1, 0, 999, 2000):
-        got = run_select_agg(ctx, cols, n, bound)
+        got = run_select_agg(ctx, cols, n, bound, compact=compact)
         assert got == po.select_agg(f[offset:offset + n], v[offset:offset + n], bound)
 
 

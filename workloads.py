@@ -98,28 +98,44 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     ctx.gen_uniform(c0, n, 0x5EED0001, 0, 0, 1 << 31, stream=stream)
     ctx.gen_uniform(c1, n, 0x5EED0001, 1, 0, 1 << 20, stream=stream)
     head, agg = mgv.create_sum_select_pipeline(ctx, bound, 0, 1)
-    times, ktimes = [], []
+
+    def timed_steps(steps):
+        times, ktimes = [], []
+        for i in range(args.warmup + steps):
+            with torch.cuda.stream(stream):
+                torch.sum(flush, dim=0, out=flush_out)  # inputs come from HBM every step
+            e0, e1 = _events(torch)
+            k0, k1 = _events(torch)
+            e0.record(stream)
+            head.open(stream)
+            k0.record(stream)  # enqueued while the flush still runs: the kernel follows it directly
+            head.consume_columns([c0, c1], n, stream)
+            k1.record(stream)
+            head.close(stream)
+            e1.record(stream)
+            stream.synchronize()
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1) / 1000.0)
+                ktimes.append(k0.elapsed_time(k1) / 1000.0)
+        return times, ktimes
+
     launches0 = ctx.launches
     h0 = time.time()
-    for i in range(args.warmup + args.steps):
-        with torch.cuda.stream(stream):
-            torch.sum(flush, dim=0, out=flush_out)  # inputs come from HBM every step
-        e0, e1 = _events(torch)
-        k0, k1 = _events(torch)
-        e0.record(stream)
-        head.open(stream)
-        k0.record(stream)  # enqueued while the flush still runs: the kernel follows it directly
-        head.consume_columns([c0, c1], n, stream)
-        k1.record(stream)
-        head.close(stream)
-        e1.record(stream)
-        stream.synchronize()
-        if i >= args.warmup:
-            times.append(e0.elapsed_time(e1) / 1000.0)
-            ktimes.append(k0.elapsed_time(k1) / 1000.0)
+    times, ktimes = timed_steps(args.steps)
     clk.mark(h0, time.time())
     launches = (ctx.launches - launches0) * args.steps // (args.warmup + args.steps)
     cnt, s = agg.result()
+    # the same select through the warp-ballot compaction (qualifying rows packed
+    # into 128-row vectors that the aggregate reads): untimed for the headline
+    tuning0 = ctx.tuning()
+    ctx.set_tuning(select_compact=1)
+    try:
+        _, ballot_kt = timed_steps(max(10, args.steps))
+        ballot_res = agg.result()
+    finally:
+        ctx.set_tuning(select_compact=tuning0.select_compact)
+    assert ballot_res == (cnt, s), "the warp-ballot select differs from the masked fold"
+    bkt = statistics.median(ballot_kt)
     del flush, flush_out
     t = statistics.median(times)
     kt = statistics.median(ktimes)
@@ -156,6 +172,10 @@ def run_select(args, mgv, torch, ctx, bench, clk, emit=True):
     extra = {"roofline": {"bound": "hbm", "achieved": 8 * n / kt / 1e9, "peak": peak, "unit": "GB/s",
                           "frac": 8 * n / kt / 1e9 / peak, "peak_kind": kind, "kernel_ms": 1000 * kt,
                           "algorithmic_bytes_per_launch": 8 * n, "kernel": "k_select_agg"},
+             "ballot_path": {"kernel": "k_chain<select, aggregate> (warp-ballot compaction into 128-row vectors; "
+                                       "mgv_tuning.select_compact = 1)", "kernel_ms": 1000 * bkt,
+                             "achieved_gbs": 8 * n / bkt / 1e9, "frac": 8 * n / bkt / 1e9 / peak,
+                             "checked": "COUNT and SUM equal the masked fold's (and so the oracle's)"},
              "step_gbs": 8 * n / t / 1e9,
              "e2e": {"value": n / e2e_t, "unit": "rows/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 16,
                      "ms_per_step": 1000 * e2e_t, "h2d_gbs": 8 * n / e2e_t / 1e9, "h2d_peak_gbs": h2d,
@@ -435,38 +455,63 @@ def run_batched(args, mgv, torch, ctx, bench, clk, emit=True):
     return {"value": nq / tb, "unit": "queries/s", "ms": 1000 * tb, "workload": workload, **extra}
 
 
-def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
-    """Served throughput and p50 / p99 vs the plain server; prints its line when emit, returns its figures."""
+def run_served(args, mgv, torch, ctx, bench, clk, emit=True, mix="sizes"):
+    """Served throughput and p50 / p99 vs the plain server; prints its line when emit, returns its figures.
+
+    mix "sizes": requests of the batched mix's sizes over 16 resident tables.
+    mix "config3": the config-3 query (select filter <= b -> join on 2^24
+    build keys -> group-by Zipf(1) over 4096 groups, 2^27 probe rows) with
+    the bound b uniform in [9, 199] (selectivity 1 % to 20 %, 10 % on
+    average) over the one resident config-3 table, so that the requests of a
+    batch share their scan."""
     import numpy as np
 
     stream = torch.cuda.Stream()
-    ntab = 16
-    rng = np.random.default_rng(0x5EED0005)
-    prows = 1 << 24
     tables = []
-    for t in range(ntab):
-        nb = int(2 ** rng.uniform(10, 22))
-        g = int(2 ** rng.uniform(4, 16))
+    if mix == "config3":
+        ntab = 1
+        nb, prows, g, seed = 1 << 24, 1 << 27, 4096, 0x5EED0003
         with torch.cuda.stream(stream):
             bk = torch.empty(nb, dtype=torch.int32, device="cuda")
             cols = [torch.empty(prows, dtype=torch.int32, device="cuda") for _ in range(4)]
-        s = 0x5EED0005 * 100 + t
-        ctx.gen_perm(bk, nb, s, stream=stream)
-        ctx.gen_probe_keys(cols[0], prows, s + 1, s, nb, HIT, nb, (1 << 31) - nb, stream=stream)
-        ctx.gen_uniform(cols[1], prows, s + 1, 2, 0, 1000, stream=stream)
-        ctx.gen_zipf(cols[2], prows, s + 1, 3, g, stream=stream)
-        ctx.gen_uniform(cols[3], prows, s + 1, 4, 0, 1 << 20, stream=stream)
+        ctx.gen_perm(bk, nb, seed, stream=stream)
+        ctx.gen_uniform(cols[0], prows, seed, 1, 0, nb, stream=stream)
+        ctx.gen_uniform(cols[1], prows, seed, 2, 0, 1000, stream=stream)
+        ctx.gen_zipf(cols[2], prows, seed, 3, g, stream=stream)
+        ctx.gen_uniform(cols[3], prows, seed, 4, 0, 1 << 16, stream=stream)
         tables.append((nb, g, bk, cols))
+        seconds, burst = args.serve_seconds_config3, args.saturate_config3
+    else:
+        ntab = 16
+        rng = np.random.default_rng(0x5EED0005)
+        prows = 1 << 24
+        for t in range(ntab):
+            nb = int(2 ** rng.uniform(10, 22))
+            g = int(2 ** rng.uniform(4, 16))
+            with torch.cuda.stream(stream):
+                bk = torch.empty(nb, dtype=torch.int32, device="cuda")
+                cols = [torch.empty(prows, dtype=torch.int32, device="cuda") for _ in range(4)]
+            s = 0x5EED0005 * 100 + t
+            ctx.gen_perm(bk, nb, s, stream=stream)
+            ctx.gen_probe_keys(cols[0], prows, s + 1, s, nb, HIT, nb, (1 << 31) - nb, stream=stream)
+            ctx.gen_uniform(cols[1], prows, s + 1, 2, 0, 1000, stream=stream)
+            ctx.gen_zipf(cols[2], prows, s + 1, 3, g, stream=stream)
+            ctx.gen_uniform(cols[3], prows, s + 1, 4, 0, 1 << 20, stream=stream)
+            tables.append((nb, g, bk, cols))
+        seconds, burst = args.serve_seconds, args.saturate
     stream.synchronize()
     rates = [float(r) for r in args.rates.split(",")]
 
     def trace(rate, seed):
-        """Arrival times and requests; rate 0 = a burst of --saturate requests at once."""
+        """Arrival times and requests; rate 0 = a burst of `burst` requests at once."""
         r = np.random.default_rng(seed)
-        n = max(1, int(rate * args.serve_seconds)) if rate else args.saturate
+        n = max(1, int(rate * seconds)) if rate else burst
         gaps = r.exponential(1.0 / rate, n) if rate else np.zeros(n)
         reqs = []
         for i in range(n):
+            if mix == "config3":
+                reqs.append((0, prows, int(r.integers(9, 200))))
+                continue
             t = int(r.integers(ntab))
             rows = int(2 ** r.uniform(12, 24))
             bound = int(round(r.uniform(0.01, 0.90) * 1000)) - 1
@@ -483,7 +528,8 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
         # warm-up: a burst of the mix, so the server's device regions and pinned
         # landing zones have grown to steady-state sizes before anything is timed
         _, warm = trace(0.0, seed + 777)
-        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1]) for t, rows, bound in warm[:512]]
+        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1])
+                   for t, rows, bound in warm[:512 if mix == "sizes" else 64]]
         wbuf = (mgv.GroupRow * (1 << 16))()
         wn, wlat = ctypes.c_uint64(), ctypes.c_double()
         for tk in tickets:
@@ -544,36 +590,61 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True):
         digests = []
         for i in range(len(reqs)):
             rows = res[offs[i]:offs[i] + got[i]]
-            mix = rows[:, 0] * np.uint64(0x9E3779B97F4A7C15) ^ rows[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F) \
+            hsh = rows[:, 0] * np.uint64(0x9E3779B97F4A7C15) ^ rows[:, 1] * np.uint64(0xC2B2AE3D27D4EB4F) \
                 ^ rows[:, 2] * np.uint64(0x165667B19E3779F9)
-            digests.append((got[i], int(mix.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(mix)) if got[i] else 0))
+            digests.append((got[i], int(hsh.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(hsh)) if got[i] else 0))
         stats = srv.stats()
         srv.destroy()
         return {"offered_qps": rate or None, "arrived_qps": len(reqs) / t_sub, "requests": len(reqs),
                 "throughput_qps": len(reqs) / wall, "p50_ms": stats.p50_ms, "p99_ms": stats.p99_ms,
                 "mean_ms": stats.mean_ms, "max_ms": stats.max_ms, "batches": stats.batches,
-                "mean_batch": stats.mean_batch, "peak_device_bytes": stats.peak_bytes}, digests
+                "mean_batch": stats.mean_batch, "shared_scans": stats.shared_scans,
+                "scan_queries": stats.scan_queries, "peak_device_bytes": stats.peak_bytes}, digests, reqs, res, offs, got
 
     sys.setswitchinterval(2e-4)  # the submitting and draining threads share the GIL
     out = []
     h0 = time.time()
     for k, rate in enumerate(rates + [0.0]):
         if getattr(args, "served_plain_first", False):
-            p, rp = serve(True, rate, 1000 + k)
-            b, rb = serve(False, rate, 1000 + k)
+            p, rp, *_ = serve(True, rate, 1000 + k)
+            b, rb, breqs, bres, boffs, bgot = serve(False, rate, 1000 + k)
         else:
-            b, rb = serve(False, rate, 1000 + k)
-            p, rp = serve(True, rate, 1000 + k)
+            b, rb, breqs, bres, boffs, bgot = serve(False, rate, 1000 + k)
+            p, rp, *_ = serve(True, rate, 1000 + k)
         assert rb == rp, "served results differ from the plain server"
         out.append({"rate": rate if rate else "saturated", "batched": b, "plain": p})
     clk.mark(h0, time.time())
+    checked = "every request's result equals the plain server's"
+    if mix == "config3":
+        # two requests of the burst against the oracle as well (all host threads)
+        import pyoracle as po
+
+        nb, g, bk, cols = tables[0]
+        hb = bk.cpu().numpy()
+        hc = [c.cpu().numpy() for c in cols]
+        for i in (0, len(breqs) - 1):
+            _, rows, bound = breqs[i]
+            want, _, _ = po.run_query(hb, hc[0][:rows], hc[1][:rows], hc[2][:rows], hc[3][:rows], bound,
+                                      os.cpu_count() or 1)
+            rws = bres[boffs[i]:boffs[i] + bgot[i]].view(np.int64)  # mgv_group_row: group (+ pad), sum, count
+            gotr = [(((int(a) & 0xFFFFFFFF) ^ 0x80000000) - 0x80000000, int(b_), int(c)) for a, b_, c in rws]
+            assert sorted(gotr) == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want], \
+                "served config-3 request differs from the oracle"
+        checked += "; two requests of the burst equal the oracle's select -> join -> group-by over 2^27 rows"
     sat = out[-1]
-    workload = ("open-loop Poisson arrivals of the batched mix over 16 resident tables (build 2^U(10,22), probe "
-                "2^U(12,24) rows, selectivity U(1%,90%), groups 2^U(4,16)) at each rate, then a burst of "
-                f"{args.saturate} requests (saturated); 40 GB budget; continuous batching")
+    if mix == "config3":
+        workload = ("open-loop Poisson arrivals of config-3 queries (select filter <= b, b uniform in [9, 199]: "
+                    "selectivity 1-20 %, 10 % on average -> join on 2^24 resident build keys -> group-by Zipf(1) "
+                    "over 4096 groups, 2^27 probe rows each) for "
+                    f"{seconds} s at each rate, then a burst of {burst} requests (saturated); 40 GB budget; "
+                    "continuous batching with shared scans")
+    else:
+        workload = ("open-loop Poisson arrivals of the batched mix over 16 resident tables (build 2^U(10,22), probe "
+                    "2^U(12,24) rows, selectivity U(1%,90%), groups 2^U(4,16)) at each rate, then a burst of "
+                    f"{burst} requests (saturated); 40 GB budget; continuous batching")
     extra = {"rates": out[:-1], "saturated": sat,
              "saturated_speedup_vs_plain": sat["batched"]["throughput_qps"] / sat["plain"]["throughput_qps"],
-             "checked": "every request's result equals the plain server's"}
+             "checked": checked}
     if emit:
         _line(args, "served queries/s & p99 latency vs plain", sat["batched"]["throughput_qps"], "queries/s",
               sat["batched"]["mean_ms"], workload, extra, clk)
@@ -593,7 +664,8 @@ def run(args) -> int:
     ctx = mgv.Context(int(os.environ.get("LOCAL_RANK", "0")))
     fn = {"select": run_select, "pipeline": run_pipeline, "batched": run_batched, "served": run_served,
           "delivery": run_delivery}[args.workload]
+    kw = {"mix": args.served_mix} if args.workload == "served" else {}
     with bench.ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-        fn(args, mgv, torch, ctx, bench, clk)
+        fn(args, mgv, torch, ctx, bench, clk, **kw)
     ctx.close()
     return 0
