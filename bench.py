@@ -315,6 +315,8 @@ def main():
     ap.add_argument("--saturate", type=int, default=5000, help="served: requests in the closing burst")
     ap.add_argument("--served-mix", default="sizes", choices=["sizes", "config3"],
                     help="served: the batched mix's sizes over 16 tables, or config-3 queries over one table")
+    ap.add_argument("--served-burst-only", action="store_true",
+                    help="served: only the batched server's closing burst (no rates, no plain server)")
     ap.add_argument("--serve-seconds-config3", type=float, default=0.5,
                     help="served config-3 mix: arrival window per rate")
     ap.add_argument("--saturate-config3", type=int, default=1000,

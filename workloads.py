@@ -525,11 +525,12 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True, mix="sizes"):
 
         srv = mgv.Server(ctx, 40 << 30, max_batch=256, max_inflight=2, plain=plain)
         tids = [srv.add_table(bk, nb) for nb, g, bk, cols in tables]
-        # warm-up: a burst of the mix, so the server's device regions and pinned
-        # landing zones have grown to steady-state sizes before anything is timed
+        # warm-up: a burst of the mix (two full batches and more), so the server's
+        # device regions and pinned landing zones have grown to steady-state
+        # sizes before anything is timed (pinning a zone of a full batch's
+        # rows takes 10-15 ms, more on a fresh host)
         _, warm = trace(0.0, seed + 777)
-        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1])
-                   for t, rows, bound in warm[:512 if mix == "sizes" else 64]]
+        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1]) for t, rows, bound in warm[:512]]
         wbuf = (mgv.GroupRow * (1 << 16))()
         wn, wlat = ctypes.c_uint64(), ctypes.c_double()
         for tk in tickets:
@@ -604,7 +605,14 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True, mix="sizes"):
     sys.setswitchinterval(2e-4)  # the submitting and draining threads share the GIL
     out = []
     h0 = time.time()
+    burst_only = getattr(args, "served_burst_only", False)
+    if burst_only:
+        rates = []
     for k, rate in enumerate(rates + [0.0]):
+        if burst_only:  # the batched server's burst alone (for launch lists), checked against the oracle below
+            b, rb, breqs, bres, boffs, bgot = serve(False, rate, 1000 + k)
+            out.append({"rate": "saturated", "batched": b, "plain": b})
+            continue
         if getattr(args, "served_plain_first", False):
             p, rp, *_ = serve(True, rate, 1000 + k)
             b, rb, breqs, bres, boffs, bgot = serve(False, rate, 1000 + k)
