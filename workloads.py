@@ -525,12 +525,16 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True, mix="sizes"):
 
         srv = mgv.Server(ctx, 40 << 30, max_batch=256, max_inflight=2, plain=plain)
         tids = [srv.add_table(bk, nb) for nb, g, bk, cols in tables]
-        # warm-up: a burst of the mix (two full batches and more), so the server's
-        # device regions and pinned landing zones have grown to steady-state
-        # sizes before anything is timed (pinning a zone of a full batch's
-        # rows takes 10-15 ms, more on a fresh host)
+        # warm-up: a burst of the mix (four full batches), so the server's device
+        # regions and pinned landing zones have grown to their steady-state sizes
+        # and number before anything is timed (pinning a zone for a full batch's
+        # rows takes 10-60 ms, and a burst keeps three or four zones in use: two
+        # batches in flight, one or two whose requests are still being waited for)
         _, warm = trace(0.0, seed + 777)
-        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1]) for t, rows, bound in warm[:512]]
+        nwarm = 1024
+        while len(warm) < nwarm:
+            warm = warm + warm
+        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1]) for t, rows, bound in warm[:nwarm]]
         wbuf = (mgv.GroupRow * (1 << 16))()
         wn, wlat = ctypes.c_uint64(), ctypes.c_double()
         for tk in tickets:
