@@ -371,3 +371,61 @@ def test_shared_memory_build_unique_keys(ctx, torch_cuda):
     cnt, s, info = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
     assert info.has_duplicates == 0 and info.rows == 1 << 20
     assert cnt == hits and (cnt, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+
+
+MN, MX = -(1 << 31), (1 << 31) - 1
+
+
+@pytest.mark.parametrize("tuned", [PROBE_VARIANTS[0], PROBE_VARIANTS[1], PROBE_VARIANTS[4], PROBE_VARIANTS[6]],
+                         indirect=True, ids=lambda v: "_".join(f"{k[6:]}{x}" for k, x in v.items()))
+@pytest.mark.parametrize("case", ["spread", "extremes", "only_reserved", "narrow", "negative"])
+def test_probe_keys_around_the_build_range(ctx, torch_cuda, tuned, case):
+    """Probe keys at, just inside and just outside both ends of the build
+    keys' range, INT32_MIN (the side list) and INT32_MAX, and a build of
+    reserved keys only, all against the oracle."""
+    rng = np.random.default_rng(sum(map(ord, case)))
+    if case == "spread":
+        bk = rng.integers(-1000, 1000, 40000).astype(np.int32)
+    elif case == "extremes":
+        bk = rng.integers(-50, 50, 30000).astype(np.int32)
+        bk[:4] = [MN, MX, MN + 1, MX - 1]
+    elif case == "only_reserved":
+        bk = np.full(5000, MN, np.int32)
+    elif case == "narrow":
+        bk = np.full(70000, 12345, np.int32)
+        bk[::3] = 12346
+    else:
+        bk = rng.integers(-(1 << 30), -(1 << 29), 100000).astype(np.int32)
+    lo = int(bk[bk != MN].min()) if (bk != MN).any() else 0
+    hi = int(bk[bk != MN].max()) if (bk != MN).any() else 0
+    edge = np.array([lo - 1, lo, lo + 1, hi - 1, hi, hi + 1, MN, MX, MN + 1, MX - 1, 0], np.int64)
+    edge = np.clip(edge, MN, MX).astype(np.int32)
+    pk = np.concatenate([rng.integers(MN, MX, 300000, dtype=np.int64).astype(np.int32),
+                         rng.choice(bk, 300000), np.tile(edge, 1000)])
+    pk = pk[rng.permutation(pk.size)]
+    bp = rng.integers(MN, MX, bk.size, dtype=np.int64).astype(np.int32)
+    pp = rng.integers(MN, MX, pk.size, dtype=np.int64).astype(np.int32)
+    c, s, _ = join_count_sum(ctx, torch_cuda, bk, bp, pk, pp)
+    assert (c, s) == po.Chain(bk, bp).probe_agg(pk, pp)
+
+
+def test_reopened_build_with_other_keys(ctx, torch_cuda):
+    """One build operator reopened three times, each time with keys in another
+    range, probed after each build."""
+    torch = torch_cuda
+    bhead, hb, probe, agg = mgv.create_count_join_1G_pipeline(ctx, 100000)
+    pk = np.arange(-10000, 20000, dtype=np.int32)
+    pp = np.ones(pk.size, np.int32)
+    dpk, dpp = dev(torch, pk), dev(torch, pp)
+    for lo in (0, 5000, -9000):
+        bk = np.arange(lo, lo + 1000, dtype=np.int32)
+        bp = np.full(bk.size, 7, np.int32)
+        bhead.open()
+        bhead.consume_columns([dev(torch, bk), dev(torch, bp)], bk.size)
+        bhead.close()
+        probe.open()
+        probe.consume_columns([dpk, dpp], pk.size)
+        probe.close()
+        assert agg.result() == po.Chain(bk, bp).probe_agg(pk, pp) == (1000, 8000)
+    for o in (probe, agg, bhead, hb):
+        o.destroy()
