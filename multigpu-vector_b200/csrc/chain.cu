@@ -274,17 +274,19 @@ __device__ __forceinline__ void smem_groups_flush(const SmemGroups& sg, const Gr
 
 // ---- shared scans: per-(range, group) cells ------------------------------------
 //
-// A CTA's shared cell table, keyed by (range << 32) | group in 64 bits
-// (EMPTY = ~0, which no range below 2^31 produces); count and the biased
-// two-word sum as in SmemGroups.  Cells that find no shared slot go to the
-// range's global table, which shares its key array (the group directory)
-// with every other range (CellsView).
+// A CTA's shared cell table, keyed by (range << 21) | group in 32 bits for
+// groups in [0, 2^21 - 1) (EMPTY = ~0, which no such key produces), with a
+// count and the biased two-word sum as in SmemGroups: 16 bytes a slot, so
+// 8192 slots fit beside the rings.  Cells of other groups, and cells that
+// find no shared slot, go to the range's global table, which shares its key
+// array (the group directory) with every other range (CellsView).
 
-constexpr uint32_t kCellSlots = 4096;  // shared cells per CTA (80 KiB)
-constexpr unsigned long long kEmptyCell = ~0ull;
+constexpr uint32_t kCellSlots = 8192;  // shared cells per CTA (128 KiB)
+constexpr uint32_t kEmptyCell = 0xFFFFFFFFu;
+constexpr uint32_t kCellGroupBits = 21;  // range index above, group below
 
 struct SmemCells {
-    unsigned long long* keys;
+    uint32_t* keys;
     uint32_t* cnt;
     uint32_t* lo;
     uint32_t* hi;
@@ -292,12 +294,12 @@ struct SmemCells {
     uint32_t cap;  // power of two
 };
 
-__host__ __device__ __forceinline__ size_t smem_cells_bytes(uint32_t cap) { return (size_t)cap * 20 + 16; }
+__host__ __device__ __forceinline__ size_t smem_cells_bytes(uint32_t cap) { return (size_t)cap * 16 + 16; }
 
 __device__ __forceinline__ SmemCells smem_cells_at(unsigned char* base, uint32_t cap) {
     SmemCells c;
-    c.keys = reinterpret_cast<unsigned long long*>(base);
-    c.cnt = reinterpret_cast<uint32_t*>(base + (size_t)cap * 8);
+    c.keys = reinterpret_cast<uint32_t*>(base);
+    c.cnt = c.keys + cap;
     c.lo = c.cnt + cap;
     c.hi = c.lo + cap;
     c.used = c.hi + cap;
@@ -305,12 +307,12 @@ __device__ __forceinline__ SmemCells smem_cells_at(unsigned char* base, uint32_t
     return c;
 }
 
-__device__ __forceinline__ uint32_t cell_hash(unsigned long long key, uint32_t cap) {
-    return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (33 + __clz(cap)));  // cap = 2^k: shift = 64 - k
+__device__ __forceinline__ uint32_t cell_hash(uint32_t key, uint32_t cap) {
+    return (key * 2654435769u) >> (__clz(cap) + 1);  // cap = 2^k: shift = 32 - k
 }
 
 // Range of a filter value that passed the select (f <= b[m-1]): the first j
-// with b[j] >= f.
+// with b[j] >= f, by binary search.
 __device__ __forceinline__ uint32_t cell_range(const int32_t* b, uint32_t m, int32_t f) {
     uint32_t lo = 0, hi = m - 1;
     while (lo < hi) {
@@ -324,24 +326,26 @@ __device__ __forceinline__ uint32_t cell_range(const int32_t* b, uint32_t m, int
 // One matched row (g, v) of range j, per lane.
 __device__ __forceinline__ void cells_add_row(const SmemCells& sc, const CellsView& cv, uint32_t j, int32_t g,
                                               int32_t v, uint32_t* err) {
-    const unsigned long long key = ((unsigned long long)j << 32) | (uint32_t)g;
-    uint32_t slot = cell_hash(key, sc.cap);
+    if ((uint32_t)g < (1u << kCellGroupBits) - 1u) {
+        const uint32_t key = (j << kCellGroupBits) | (uint32_t)g;
+        uint32_t slot = cell_hash(key, sc.cap);
 #pragma unroll 1
-    for (uint32_t i = 0; i < kGroupProbes; ++i) {
-        unsigned long long k = *((volatile unsigned long long*)(sc.keys + slot));
-        if (k == kEmptyCell) {
-            if (*(volatile uint32_t*)sc.used >= smem_groups_limit(sc.cap)) break;  // stays global
-            k = atomicCAS(sc.keys + slot, kEmptyCell, key);
-            if (k == kEmptyCell) atomicAdd(sc.used, 1u);
+        for (uint32_t i = 0; i < kGroupProbes; ++i) {
+            uint32_t k = *((volatile uint32_t*)(sc.keys + slot));
+            if (k == kEmptyCell) {
+                if (*(volatile uint32_t*)sc.used >= smem_groups_limit(sc.cap)) break;  // stays global
+                k = atomicCAS(sc.keys + slot, kEmptyCell, key);
+                if (k == kEmptyCell) atomicAdd(sc.used, 1u);
+            }
+            if (k == kEmptyCell || k == key) {
+                const uint32_t x = (uint32_t)v ^ 0x80000000u;  // v + 2^31
+                atomicAdd(sc.cnt + slot, 1u);
+                const uint32_t old = atomicAdd(sc.lo + slot, x);
+                if (old + x < old) atomicAdd(sc.hi + slot, 1u);
+                return;
+            }
+            slot = (slot + 1) & (sc.cap - 1);
         }
-        if (k == kEmptyCell || k == key) {
-            const uint32_t x = (uint32_t)v ^ 0x80000000u;  // v + 2^31
-            atomicAdd(sc.cnt + slot, 1u);
-            const uint32_t old = atomicAdd(sc.lo + slot, x);
-            if (old + x < old) atomicAdd(sc.hi + slot, 1u);
-            return;
-        }
-        slot = (slot + 1) & (sc.cap - 1);
     }
     global_group_add(cells_range(cv, j), g, (unsigned long long)(long long)v, 1ull, err);
 }
@@ -360,19 +364,30 @@ __device__ __forceinline__ void smem_cells_flush(const SmemCells& sc, const Cell
     for (uint32_t i = threadIdx.x; i < sc.cap; i += blockDim.x) {
         const uint32_t c = sc.cnt[i];
         if (c == 0) continue;
-        const unsigned long long key = sc.keys[i];
+        const uint32_t key = sc.keys[i];
         const unsigned long long biased = ((unsigned long long)sc.hi[i] << 32) | sc.lo[i];
-        global_group_add(cells_range(cv, (uint32_t)(key >> 32)), (int32_t)(uint32_t)key,
+        global_group_add(cells_range(cv, key >> kCellGroupBits),
+                         (int32_t)(key & ((1u << kCellGroupBits) - 1u)),
                          biased - ((unsigned long long)c << 31), (unsigned long long)c, err);
     }
 }
 
 // What a shared scan's chain needs besides the descriptor: the CTA's cell
-// table and the bounds, copied to shared memory.
+// table, the bounds and the range lookup table, copied to shared memory.
 struct CellCtx {
     SmemCells sc;
     const int32_t* bounds;
+    const uint16_t* lut;
+    uint32_t lut_len;
+    int32_t lut_base;
 };
+
+// The same from the scan's lookup table when f lies in [lut_base, lut_base +
+// lut_len) -- the span of the bounds, when it is short -- else by search.
+__device__ __forceinline__ uint32_t cell_range_of(const CellCtx& cc, uint32_t m, int32_t f) {
+    const uint32_t d = (uint32_t)f - (uint32_t)cc.lut_base;
+    return d < cc.lut_len ? (uint32_t)cc.lut[d] : cell_range(cc.bounds, m, f);
+}
 
 // ---- the chain: per-warp processing of a row range ------------------------------
 
@@ -573,7 +588,7 @@ __device__ __forceinline__ void chain_windows(const ChainDev& a, bool unique, ui
             const unsigned m = __ballot_sync(0xffffffffu, pass);
             if (pass) {
                 uint32_t e = row;
-                if (TERM == kTermCells) e |= cell_range(cc->bounds, a.cells.m, f[k]) << kCellRowBits;
+                if (TERM == kTermCells) e |= cell_range_of(*cc, a.cells.m, f[k]) << kCellRowBits;
                 ids[(head + fill + __popc(m & lt)) & (kIdRing - 1)] = e;
             }
             fill += __popc(m);
@@ -688,7 +703,11 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_cells(const ChainDev* 
     CellCtx cc;
     cc.sc = smem_cells_at(smem_raw + kRingBytes, kCellSlots);
     int32_t* sb = reinterpret_cast<int32_t*>(smem_raw + kRingBytes + smem_cells_bytes(kCellSlots));
+    uint16_t* sl = reinterpret_cast<uint16_t*>(sb + kMaxCellRanges);
     cc.bounds = sb;
+    cc.lut = sl;
+    cc.lut_len = 0;
+    cc.lut_base = 0;
 
     int64_t cur = -1;
     unsigned long long acnt = 0, asum = 0;
@@ -705,6 +724,9 @@ __global__ void __launch_bounds__(kChainBlock, 1) k_batch_cells(const ChainDev* 
                 reinterpret_cast<uint32_t*>(&sq)[i] = reinterpret_cast<const uint32_t*>(qs + cur)[i];
             const CellsView cv = qs[cur].cells;
             for (uint32_t i = threadIdx.x; i < cv.m; i += kChainBlock) sb[i] = cv.bounds[i];
+            for (uint32_t i = threadIdx.x; i < cv.lut_len; i += kChainBlock) sl[i] = cv.lut[i];
+            cc.lut_len = cv.lut_len;
+            cc.lut_base = cv.lut_base;
             smem_cells_init(cc.sc);
             __syncthreads();
         }
@@ -737,7 +759,8 @@ __global__ void k_cells_prefix(unsigned long long* __restrict__ vals, uint64_t w
 cudaError_t launch_cells(const ChainDev* d_scans, const BatchItem* items, uint32_t nitems, cudaStream_t s,
                          Context* ctx) {
     if (nitems == 0) return cudaSuccess;
-    const size_t smem = kRingBytes + smem_cells_bytes(kCellSlots) + sizeof(int32_t) * kMaxCellRanges;
+    const size_t smem = kRingBytes + smem_cells_bytes(kCellSlots) + sizeof(int32_t) * kMaxCellRanges +
+                        sizeof(uint16_t) * kCellLut;
     cudaError_t e = cudaFuncSetAttribute(k_batch_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (int)std::min<uint64_t>((uint64_t)ctx->prop.multiProcessorCount, nitems);

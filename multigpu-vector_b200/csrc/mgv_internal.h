@@ -241,9 +241,13 @@ struct CellsView {
     uint32_t cap;                // directory slots, power of two
     int32_t* keys;               // the group directory (EMPTY = INT32_MIN)
     unsigned long long* vals;    // m blocks of [sums (cap) | counts (cap) | special sum, count]
+    const uint16_t* lut;         // range of filter value lut_base + i, i < lut_len (0: none)
+    uint32_t lut_len;
+    int32_t lut_base;
 };
 constexpr uint32_t kCellRowBits = 20;        // ring entries: row offset (low bits) | range (high bits)
 constexpr uint32_t kMaxCellRanges = 2048;    // distinct bounds per shared scan (range index < 2^11)
+constexpr uint32_t kCellLut = 8192;          // longest range lookup table (filter values b[0]..b[m-1])
 __host__ __device__ __forceinline__ size_t cell_block_words(uint32_t cap) { return 2ull * cap + 2; }
 __host__ __device__ __forceinline__ GroupTableView cells_range(const CellsView& c, uint32_t j) {
     GroupTableView g;

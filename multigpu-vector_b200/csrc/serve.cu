@@ -188,8 +188,9 @@ struct Scan {
     std::vector<uint32_t> reqs;
     std::vector<int32_t> bounds;
     std::vector<uint32_t> rank;  // per entry of reqs
+    std::vector<uint16_t> lut;   // range of filter value bounds[0] + i, when the bounds span <= kCellLut values
     uint32_t cap = 0;
-    size_t dir_off = 0, vals_off = 0, bounds_off = 0;
+    size_t dir_off = 0, vals_off = 0, bounds_off = 0, lut_off = 0;
 };
 
 // Launch one batch of admitted requests on slot `sl` (scheduler thread, lock
@@ -227,6 +228,15 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
                     sc.rank.push_back((uint32_t)(std::lower_bound(sc.bounds.begin(), sc.bounds.end(),
                                                                   sl.reqs[i]->r.filter_bound) -
                                                  sc.bounds.begin()));
+                const int64_t span = (int64_t)sc.bounds.back() - sc.bounds.front() + 1;
+                if (span <= (int64_t)kCellLut) {
+                    sc.lut.resize((size_t)span);
+                    uint16_t j = 0;
+                    for (int64_t d = 0; d < span; ++d) {  // the first j with bounds[j] >= bounds[0] + d
+                        while ((int64_t)sc.bounds[j] < (int64_t)sc.bounds.front() + d) ++j;
+                        sc.lut[(size_t)d] = j;
+                    }
+                }
                 for (uint32_t i : sc.reqs) scan_of[i] = (int32_t)scans.size();
                 scans.push_back(std::move(sc));
             }
@@ -296,6 +306,9 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     for (Scan& sc : scans) {
         sc.bounds_off = off;
         off += 4ull * sc.bounds.size();
+        sc.lut_off = off;
+        off += 2ull * sc.lut.size();
+        off = (off + 3) & ~(size_t)3;
     }
     off = align256(off);
 
@@ -345,7 +358,9 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
         hs[g].sel_bound = sc.bounds.back();
         hs[g].cells = CellsView{reinterpret_cast<const int32_t*>(A + sc.bounds_off), (uint32_t)sc.bounds.size(),
                                 sc.cap, reinterpret_cast<int32_t*>(A + sc.dir_off),
-                                reinterpret_cast<unsigned long long*>(A + sc.vals_off)};
+                                reinterpret_cast<unsigned long long*>(A + sc.vals_off),
+                                reinterpret_cast<const uint16_t*>(A + sc.lut_off), (uint32_t)sc.lut.size(),
+                                sc.bounds.front()};
     }
     std::vector<uint32_t> rank_of(nq, 0);
     for (const Scan& sc : scans)
@@ -391,6 +406,8 @@ mgv_status launch(mgv_server* S, Inflight& sl) {
     if (!si.empty()) std::memcpy(sl.hdesc + (si_off - qs_off), si.data(), sizeof(BatchItem) * si.size());
     for (const Scan& sc : scans)
         std::memcpy(sl.hdesc + (sc.bounds_off - qs_off), sc.bounds.data(), 4 * sc.bounds.size());
+    for (const Scan& sc : scans)
+        if (!sc.lut.empty()) std::memcpy(sl.hdesc + (sc.lut_off - qs_off), sc.lut.data(), 2 * sc.lut.size());
     MGV_CUDA_TRY(cudaMemcpyAsync(A + qs_off, sl.hdesc, desc_bytes, cudaMemcpyHostToDevice, s));
     MGV_CUDA_TRY(launch_fill_i32(reinterpret_cast<int32_t*>(A), slots, kEmptyKey, s, ctx));
     MGV_CUDA_TRY(cudaMemsetAsync(A + zero_begin, 0, zero_end - zero_begin, s));

@@ -101,3 +101,40 @@ def test_cell_range_edges():
         j = cell_range(b, f)
         assert b[j] >= f and (j == 0 or b[j - 1] < f)
     assert cell_range([7], 7) == 0 and cell_range([7], MN) == 0
+
+
+def lut_for(b, limit=8192):
+    """The server's range lookup table of a scan's sorted distinct bounds:
+    entry d = the first j with b[j] >= b[0] + d, when the bounds span at most
+    `limit` values; else none."""
+    span = b[-1] - b[0] + 1
+    if span > limit:
+        return []
+    out, j = [], 0
+    for d in range(span):
+        while b[j] < b[0] + d:
+            j += 1
+        out.append(j)
+    return out
+
+
+def range_of(b, lut, f):
+    """The kernel's lookup: the table for f in [b[0], b[0] + len), the search
+    otherwise (unsigned 32-bit difference, as on the device)."""
+    d = (f - b[0]) & 0xFFFFFFFF
+    return lut[d] if d < len(lut) else cell_range(b, f)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_range_lookup_table_equals_the_search(seed):
+    rng = np.random.default_rng(900 + seed)
+    lo = int(rng.choice([MN, -100, 0, (1 << 31) - 9000]))
+    width = int(rng.choice([1, 50, 8192, 9000]))
+    b = sorted(set(int(x) for x in rng.integers(lo, min(lo + width, (1 << 31) - 1) + 1, 40)))
+    lut = lut_for(b)
+    assert (len(lut) > 0) == (b[-1] - b[0] + 1 <= 8192)
+    fs = [MN, MN + 1, b[0] - 1, b[0], b[-1]] + [int(x) for x in rng.integers(max(MN, b[0] - 20), b[-1] + 1, 500)]
+    for f in fs:
+        if f < MN or f > b[-1]:
+            continue
+        assert range_of(b, lut, f) == cell_range(b, f), (b[:4], f)
