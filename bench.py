@@ -514,6 +514,7 @@ def served_summary(served):
     pick = ("throughput_qps", "p50_ms", "p99_ms", "mean_ms", "mean_batch", "shared_scans")
     return {"saturated_qps": served["value"], "saturated_plain_qps": served["saturated"]["plain"]["throughput_qps"],
             "saturated_speedup_vs_plain": served["saturated_speedup_vs_plain"],
+            "saturated_detail": served["saturated"],
             "rates": {str(r): {"batched": {k: at[r]["batched"][k] for k in pick},
                                "plain": {k: at[r]["plain"][k] for k in pick}} for r in at},
             "workload": served["workload"], "checked": served["checked"]}

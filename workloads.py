@@ -525,71 +525,71 @@ def run_served(args, mgv, torch, ctx, bench, clk, emit=True, mix="sizes"):
 
         srv = mgv.Server(ctx, 40 << 30, max_batch=256, max_inflight=2, plain=plain)
         tids = [srv.add_table(bk, nb) for nb, g, bk, cols in tables]
-        # warm-up: a burst of the mix (four full batches), so the server's device
-        # regions and pinned landing zones have grown to their steady-state sizes
-        # and number before anything is timed (pinning a zone for a full batch's
-        # rows takes 10-60 ms, and a burst keeps three or four zones in use: two
+        def run_trace(at, reqs):
+            """Submits `reqs` at their arrival times while a second thread waits
+            for each and lands its rows (the ctypes wait releases the GIL).  The
+            drain only waits: request i's rows land in its own slice of one
+            preallocated array (its max_groups rows), so it keeps up with the
+            server, and digests are computed after the timed region."""
+            caps = [tables[t][1] for t, _, _ in reqs]
+            offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+            res = np.empty((int(offs[-1]), 3), dtype=np.uint64)  # mgv_group_row = 3 x 64 bits
+            res.fill(0)  # its pages are faulted in here, not by the draining thread while timed
+            got = [0] * len(reqs)
+            tq: "queue.Queue[tuple[int, int] | None]" = queue.Queue()
+            errs = []
+
+            def drain():
+                n, lat = ctypes.c_uint64(), ctypes.c_double()
+                base = res.ctypes.data
+                while True:
+                    item = tq.get()
+                    if item is None:
+                        return
+                    i, tk = item
+                    st = mgv.load().mgv_server_wait(srv.h, tk, 600000, ctypes.c_void_p(base + 24 * int(offs[i])),
+                                                    caps[i], ctypes.byref(n), ctypes.byref(lat))
+                    if st != mgv.OK:
+                        errs.append(st)
+                    got[i] = min(n.value, caps[i])
+
+            th = threading.Thread(target=drain)
+            th.start()
+            k_sub = 0
+            t0 = time.perf_counter()
+            for a, (t, rows, bound) in zip(at, reqs):
+                wait = a - (time.perf_counter() - t0)
+                if wait > 1e-4:
+                    time.sleep(wait - 5e-5)  # releases the GIL for the draining thread
+                while time.perf_counter() - t0 < a:
+                    pass
+                nb_, g_, bk_, cols_ = tables[t]
+                tq.put((k_sub, srv.submit(tids[t], *cols_, rows, bound, g_)))
+                k_sub += 1
+            t_sub = time.perf_counter() - t0
+            tq.put(None)
+            th.join()
+            wall = time.perf_counter() - t0
+            return t_sub, wall, got, res, offs, errs
+
+        # warm-up: a burst of the mix (four full batches), run the way the timed
+        # burst runs (a draining thread), so the server's device regions and
+        # pinned landing zones have grown to their steady-state sizes and number
+        # before anything is timed (pinning a zone for a full batch's rows
+        # takes 10-60 ms, and a burst keeps three or four zones in use: two
         # batches in flight, one or two whose requests are still being waited for)
         _, warm = trace(0.0, seed + 777)
         nwarm = 1024
         while len(warm) < nwarm:
             warm = warm + warm
-        tickets = [srv.submit(tids[t], *tables[t][3], rows, bound, tables[t][1]) for t, rows, bound in warm[:nwarm]]
-        wbuf = (mgv.GroupRow * (1 << 16))()
-        wn, wlat = ctypes.c_uint64(), ctypes.c_double()
-        for tk in tickets:
-            st = mgv.load().mgv_server_wait(srv.h, tk, 600000, wbuf, 1 << 16, ctypes.byref(wn), ctypes.byref(wlat))
-            assert st == mgv.OK
+        assert not run_trace(np.zeros(nwarm), warm[:nwarm])[5]
         srv.reset_stats()
         # both servers start their timed window from an idle GPU: the batched
         # warm-up burst runs the GPU flat out, and its power-capped clocks
         # would otherwise still be recovering at the first timed requests
         time.sleep(0.5)
         at, reqs = trace(rate, seed)
-        # Results are drained by a second thread while requests arrive (the
-        # ctypes wait releases the GIL).  It only waits: request i's rows land
-        # in its own slice of one preallocated array (its max_groups rows), so
-        # the drain keeps up with the server, and the digests are computed
-        # after the timed region.
-        caps = [tables[t][1] for t, _, _ in reqs]
-        offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
-        res = np.empty((int(offs[-1]), 3), dtype=np.uint64)  # mgv_group_row = 3 x 64 bits
-        res.fill(0)  # its pages are faulted in here, not by the draining thread while timed
-        got = [0] * len(reqs)
-        tq: "queue.Queue[tuple[int, int] | None]" = queue.Queue()
-        errs = []
-
-        def drain():
-            n, lat = ctypes.c_uint64(), ctypes.c_double()
-            base = res.ctypes.data
-            while True:
-                item = tq.get()
-                if item is None:
-                    return
-                i, tk = item
-                st = mgv.load().mgv_server_wait(srv.h, tk, 600000, ctypes.c_void_p(base + 24 * int(offs[i])), caps[i],
-                                                ctypes.byref(n), ctypes.byref(lat))
-                if st != mgv.OK:
-                    errs.append(st)
-                got[i] = min(n.value, caps[i])
-
-        th = threading.Thread(target=drain)
-        th.start()
-        k_sub = [0]
-        t0 = time.perf_counter()
-        for a, (t, rows, bound) in zip(at, reqs):
-            wait = a - (time.perf_counter() - t0)
-            if wait > 1e-4:
-                time.sleep(wait - 5e-5)  # releases the GIL for the draining thread
-            while time.perf_counter() - t0 < a:
-                pass
-            nb, g, bk, cols = tables[t]
-            tq.put((k_sub[0], srv.submit(tids[t], *cols, rows, bound, g)))
-            k_sub[0] += 1
-        t_sub = time.perf_counter() - t0
-        tq.put(None)
-        th.join()
-        wall = time.perf_counter() - t0
+        t_sub, wall, got, res, offs, errs = run_trace(at, reqs)
         assert not errs, errs
         # order-independent digest of each request's rows (the server returns groups unordered)
         digests = []
