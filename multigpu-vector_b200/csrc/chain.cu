@@ -15,6 +15,11 @@
 // match, src/operators/hashjoin.cu:148-162); the build payload of the match
 // is visible to the terminal as column `ncols`.
 //
+// Shared scans of the query server (k_batch_cells, no reference
+// counterpart) run the same chain at the largest of several requests' filter
+// bounds and aggregate each matched row into a (filter range, group) cell;
+// a prefix over the ranges then gives each request its groups.
+//
 // Group-by (no reference counterpart): each CTA aggregates into a
 // shared-memory hash table with native 32-bit shared atomics (count, and the
 // int64 sum as two biased words).  Groups that do not find a shared slot

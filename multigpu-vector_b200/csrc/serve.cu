@@ -14,6 +14,12 @@
 // batch's pinned landing zone until each waiter copies its own rows out, so
 // the scheduler thread copies nothing and is free to launch the next batch.
 //
+// Requests of a batch over the same table, probe columns and row count that
+// differ only in their filter bound share one scan (k_batch_cells): the
+// columns are read and the table probed once, each matched row adds to the
+// cell of its filter range and group, and one prefix pass over the ranges
+// gives every request its own groups (exact: integer sums).
+//
 // With plain = 1 the server instead runs requests one at a time through the
 // operator API (select -> hash_probe -> groupby on the resident table): the
 // per-query baseline under the same arrival trace.
