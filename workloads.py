@@ -435,6 +435,25 @@ def run_batched(args, mgv, torch, ctx, bench, clk, emit=True):
             pt.append(e0.elapsed_time(e1) / 1000.0)
     mism = sum(1 for q in range(nq) if b.result(q) != b.result(q, plain=True))
     assert mism == 0, f"{mism} queries differ between batched and plain"
+    # and three queries -- the smallest, a median and the largest probe side --
+    # against the oracle's select -> join -> group-by (all host threads)
+    import pyoracle as po
+
+    by_rows = sorted(range(nq), key=lambda q: spec[q][1])
+    picked = [by_rows[0], by_rows[nq // 2], by_rows[-1]]
+    B, P = keep
+    ob = [0]
+    op = [0]
+    for nb_q, npr_q, _, _ in spec:
+        ob.append(ob[-1] + nb_q)
+        op.append(op[-1] + npr_q)
+    for q in picked:
+        nb_q, npr_q, bound_q, _ = spec[q]
+        hb = B[ob[q]:ob[q] + nb_q].cpu().numpy()
+        hp = [c[op[q]:op[q] + npr_q].cpu().numpy() for c in P]
+        want, _, _ = po.run_query(hb, hp[0], hp[1], hp[2], hp[3], bound_q, os.cpu_count() or 1)
+        assert b.result(q) == [(int(w["group"]), int(w["sum"]), int(w["count"])) for w in want], \
+            f"batched query {q} differs from the oracle"
     tb, tp = statistics.median(bt), statistics.median(pt)
     rows = sum(x[1] for x in spec)
     st = b.stats()
@@ -447,7 +466,9 @@ def run_batched(args, mgv, torch, ctx, bench, clk, emit=True):
              "batch_config": {"load_factor": cfg.load_factor, "probe_item_rows": cfg.probe_item_rows,
                               "item_order": cfg.item_order, "autotuned": not args.batch_config, "tune_s": tune_s},
              "arena_bytes": st.arena_bytes, "probe_rows": rows,
-             "probe_rows_per_s": rows / tb, "checked": "all queries equal between batched and plain"}
+             "probe_rows_per_s": rows / tb,
+             "checked": "all queries equal between batched and plain; the smallest, a median and the largest "
+                        "query (by probe rows) equal the oracle's select -> join -> group-by"}
     if emit:
         _line(args, "batched queries/s vs plain", nq / tb, "queries/s", 1000 * tb, workload, extra, clk)
     b.destroy()
